@@ -1,0 +1,486 @@
+#!/usr/bin/env python
+"""Benchmark: OSEM sub-iteration of FIR's clinical configuration on B200.
+
+A step is one OSEM sub-iteration (reconAlgos.cc:119-198) of the clinical
+workload: 32 rings x 512 crystals, R = 400 mm, LORs within a 300 mm FOV
+(3.28e7 LORs, 16 subsets of 2.05e6), 200x200x64 image at 3 mm, FWHM 4 mm
+Gaussian filter every sub-iteration, seeded synthetic phantom with water
+attenuation and 5e8 Poisson counts.  The metric counts ray-voxel steps the
+way FIR enumerates them: every path element of every LOR of the subset for
+the projection, plus every path element of the LORs whose estimate exceeds
+1e-5 for the backprojection.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fir|reference]
+
+Prints one JSON line (rank 0).  --impl reference times FIR's own OpenMP code
+(compiled from its sources into oracle/_ref) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ray-voxel steps/s fwd+bck; OSEM s/iter; batched & plain GPU vs CPU at ≤1e-4 err"
+UNIT = "ray-voxel steps/s"
+EPS = 1e-5
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=32)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", choices=["fir", "reference"], default="fir")
+    ap.add_argument("--workload", choices=["clinical", "small", "large"], default="clinical")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--block", type=int, default=0)
+    return ap.parse_args()
+
+
+def workload(name):
+    from fir_b200 import workloads
+
+    return {"clinical": workloads.clinical, "small": workloads.small, "large": workloads.large}[name]()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of the OSEM kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "osem_subset_clinical.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# -------------------------------------------------------------- step counts
+
+def subset_of_bins(proj, n_subsets, torch, device):
+    """Subset index (view % n_subsets) of every bin, flat file order."""
+    from fir_b200 import capi
+
+    g = capi.proj_geometry(proj)
+    parts = []
+    for nax in g["n_axial"]:
+        bpv = nax * g["n_tang_coords"]
+        v = torch.arange(g["n_views"], device=device, dtype=torch.int32).repeat_interleave(bpv)
+        parts.append(v % n_subsets)
+    return torch.cat(parts)
+
+
+def reference_counts(w, cache_dir="/tmp"):
+    """Path elements per bin by FIR's own Siddon (oracle/_ref, all threads)."""
+    import numpy as np
+
+    from oracle.bridge import Reference
+
+    key = f"{w.name}_{w.proj.n_rings}_{w.proj.n_crystals_per_ring}_{w.proj.n_tang_coords}_{w.vol.size[0]}"
+    path = os.path.join(cache_dir, f"fir_counts_{key}.npy")
+    if os.path.exists(path):
+        return np.load(path)
+    ref = Reference()
+    c = ref.path_counts(w.scanner, w.proj, w.vol, w.n_lors)
+    try:
+        np.save(path, c)
+    except Exception:
+        pass
+    return c
+
+
+# ------------------------------------------------------------ CPU reference
+
+def cpu_reference_run(w, steps_budget: int, verbose=False):
+    """Times FIR's reconAlgos::OSEM on host cores: `iters` full iterations
+    (16 sub-iterations each) of the clinical workload from a uniform image.
+    Measured data are seeded Poisson(15) counts and the sensitivity is
+    uniform: step counts and timing do not depend on data values, and with
+    every LOR crossing the positive image every crossing LOR is backprojected
+    (S_bwd = S_fwd)."""
+    import numpy as np
+
+    from fir_b200.geometry import OSEMParams
+    from oracle.bridge import Reference
+
+    ref = Reference()
+    cores = os.cpu_count() or 1
+    ref.threads(cores)
+    counts = reference_counts(w)
+    nb = counts.size
+    y = np.random.default_rng(w.seed).poisson(15.0, nb).astype(np.float32)
+    nsub = w.osem.n_subsets
+    sens = np.ones((nsub,) + tuple(w.vol.shape_zyx), np.float32)
+    img = np.ones(w.vol.shape_zyx, np.float32)
+    prm = OSEMParams(n_iterations=1, n_subsets=nsub, convolution_interval=w.osem.convolution_interval,
+                     fwhm_xyz=list(w.osem.fwhm_xyz), cut_radius=w.osem.cut_radius)
+    iters = max(1, int(math.ceil(steps_budget / nsub)))
+    t0 = time.perf_counter()
+    for _ in range(iters):
+        img = ref.osem(w.scanner, w.proj, w.vol, y, img, sens, prm)
+    dt = time.perf_counter() - t0
+    steps = 2 * int(counts.sum(dtype=np.int64)) * iters
+    return {
+        "value": steps / dt,
+        "unit": UNIT,
+        "cores": cores,
+        "kind": "reference",
+        "seconds": dt,
+        "osem_s_per_iteration": dt / iters,
+        "sample": f"{iters} full OSEM iteration(s) of the clinical workload ({nsub} sub-iterations each) by "
+                  f"FIR's reconAlgos::OSEM compiled -O3 -fopenmp, {cores} threads; S = {steps} ray-voxel steps",
+    }
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return 0
+    w = workload(args.workload)
+    try:
+        from oracle import bridge
+
+        if not bridge.reference_available():
+            bridge.build(reference=True)
+        if not bridge.reference_available():
+            raise FileNotFoundError("oracle/_ref/libfirref.so not built")
+    except Exception as e:  # noqa: BLE001
+        print(json.dumps({"impl": "reference", "unavailable": f"FIR reference library unavailable: {e}"}))
+        return 0
+    nsub = w.osem.n_subsets
+    budget = max(nsub, min(args.steps, 2 * nsub))
+    r = cpu_reference_run(w, budget)
+    ms = 1000.0 * r["osem_s_per_iteration"] / nsub
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": r["value"],
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 data, f64 geometry",
+        "data": "synthetic (seeded Poisson counts; uniform sensitivity)",
+        "config": {"workload": f"{w.name}: OSEM sub-iteration, 32 rings x 512 crystals, 300 mm FOV, "
+                               f"{w.n_lors} LORs, 200x200x64 @ 3 mm, {nsub} subsets, FWHM 4 mm",
+                   "osem_s_per_iteration": r["osem_s_per_iteration"]},
+        "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------ the GPU arm
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank)
+
+    import numpy as np
+    import torch
+
+    from fir_b200 import capi, workloads
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    w = workload(args.workload)
+    nsub = w.osem.n_subsets
+    nb = w.n_lors
+    nvox = w.vol.n_voxels
+    ctx = capi.Context(w.scanner, device=local)
+    aux = capi.Context(w.scanner, device=local)  # bookkeeping (untimed)
+    if w.geometry:
+        ctx.set_option(capi.FIR_OPT_GEOMETRY, w.geometry)
+        aux.set_option(capi.FIR_OPT_GEOMETRY, w.geometry)
+    if args.block:
+        ctx.set_option(capi.FIR_OPT_BLOCK_SIZE, args.block)
+
+    # ---- data: attenuated, scaled, Poisson-sampled, precorrected (OSEM.cc:294-337)
+    x_true = torch.from_numpy(workloads.activity(w)).to(dev)
+    mu = torch.from_numpy(workloads.hounsfield(w)).to(dev)
+    aux.hu_to_mu(w.vol, mu)
+    acf = torch.empty(nb, device=dev)
+    aux.forward_exp(w.vol, mu, w.proj, acf)
+    ax = torch.empty(nb, device=dev)
+    aux.forward(w.vol, x_true, w.proj, ax)
+    expected = ax / acf
+    expected *= w.counts / float(expected.sum(dtype=torch.float64))
+    gen = torch.Generator(device=dev).manual_seed(w.seed)
+    y = torch.poisson(expected, generator=gen)
+    aux.proj_multiply(w.proj, y, acf)
+    del expected, ax, x_true
+    sens = torch.empty((nsub,) + tuple(w.vol.shape_zyx), device=dev)
+    aux.sensitivity(w.proj, w.vol, sens, nsub)
+    img = torch.ones(w.vol.shape_zyx, device=dev)
+    sens_frames = [sens[s] for s in range(nsub)]
+
+    # path elements of every bin, by our own traversal (bookkeeping)
+    counts = torch.empty(nb, dtype=torch.int32, device=dev)
+    crosses = torch.empty(nb, dtype=torch.int32, device=dev)
+    bins = torch.arange(nb, dtype=torch.int64, device=dev)
+    import ctypes as C
+
+    aux.use_torch_stream()
+    capi._check(capi.lib().fir_lor_paths(aux.handle, C.byref(capi.proj_desc(w.proj)), C.byref(capi.vol_desc(w.vol, 1)),
+                                         nb, bins.data_ptr(), 0, None, None, counts.data_ptr(), crosses.data_ptr()))
+    del bins
+    subset_id = subset_of_bins(w.proj, nsub, torch, dev)
+    counts64 = counts.to(torch.int64)
+    s_fwd = [int(counts64[subset_id == s].sum()) for s in range(nsub)]
+    line = torch.empty(nb, device=dev)
+
+    def s_bwd(subset):
+        aux.forward(w.vol, img, w.proj, line)
+        m = (subset_id == subset) & (line.double() > EPS)
+        return int(counts64[m].sum())
+
+    prm = w.osem
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+
+    # ---- warm-up
+    k = 0
+    for _ in range(args.warmup):
+        ctx.osem_subiteration(w.proj, y, w.vol, img, sens_frames[k % nsub], prm, k % nsub, k + 1)
+        k += 1
+    torch.cuda.synchronize()
+    ctx.synchronize()
+
+    # ---- timed steps
+    ctx.set_option(capi.FIR_OPT_TIMING, 1)
+    ctx.projector_time(reset=True)
+    launches0 = ctx.launch_count
+    stream = torch.cuda.current_stream()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    step_counts = []
+    kernel_bytes = 0
+    gpu_id = str(local)
+    try:
+        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(gpu_id) as clocks:
+        wall0 = time.perf_counter()
+        for i in range(args.steps):
+            s = k % nsub
+            sb = s_bwd(s)
+            step_counts.append(s_fwd[s] + sb)
+            # algorithmic bytes of the fused kernel: 4 B per projection step,
+            # 8 B per backprojection step, 4 B per LOR of the subset
+            kernel_bytes += 4 * s_fwd[s] + 8 * sb + 4 * (nb // nsub)
+            flush.zero_()
+            starts[i].record(stream)
+            ctx.osem_subiteration(w.proj, y, w.vol, img, sens_frames[s], prm, s, k + 1)
+            ends[i].record(stream)
+            k += 1
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall0
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    launches = ctx.launch_count - launches0
+    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    kern_ms, kern_n = ctx.projector_time(reset=True)
+    ctx.set_option(capi.FIR_OPT_TIMING, 0)
+    total_steps = sum(step_counts)
+    if dist is not None:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t)
+    value = world * total_steps / (total_ms / 1000.0)
+
+    hbm, hbm_kind = peaks()
+    achieved = (kernel_bytes / kern_n) / (kern_ms / kern_n / 1000.0) / 1e9 if kern_n else None
+    prof = profile_traffic()
+    traffic = None
+    if prof and prof.get("dram_bytes_per_lor"):
+        traffic = prof["dram_bytes_per_lor"] * (nb // nsub)
+    roofline = {
+        "bound": "hbm",
+        "kernel": "k_osem_subset (fused projection + ratio + backprojection)",
+        "achieved": achieved,
+        "peak": hbm,
+        "unit": "GB/s",
+        "frac": achieved / hbm if achieved else None,
+        "peak_kind": f"{hbm_kind} (MEASURED_PEAKS.json hbm_gbs)" if hbm_kind == "measured" else "fallback",
+        "traffic": traffic,
+        "kernel_ms_per_launch": kern_ms / kern_n if kern_n else None,
+        "algorithmic_bytes_per_launch": kernel_bytes / max(1, kern_n),
+    }
+
+    result = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 data, f64 geometry",
+        "data": "synthetic (seeded phantom, water attenuation, Poisson counts)",
+        "config": {
+            "workload": f"{w.name}: OSEM sub-iteration, {w.proj.n_rings} rings x {w.proj.n_crystals_per_ring} "
+                        f"crystals, {w.proj.n_tang_coords} tangential bins, {nb} LORs, "
+                        f"{'x'.join(str(s) for s in w.vol.size)} @ {w.vol.voxel[0]} mm, {nsub} subsets, "
+                        f"FWHM {w.osem.fwhm_xyz[0]} mm",
+            "l2": "flushed (256 MB write) before every timed step, outside the step's events",
+            "osem_s_per_iteration": total_ms / args.steps * nsub / 1000.0,
+            "steps_per_subiteration": total_steps / args.steps,
+            "parallelism": "replicas" if world > 1 else "single GPU",
+            "wall_s_timed_loop": wall,
+        },
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "clocks": {k2: v for k2, v in clocks.summary().items() if k2 != "samples"},
+    }
+
+    # ---- end to end through the C ABI with host buffers: one OSEM iteration
+    if not args.no_e2e and rank == 0:
+        from fir_b200.geometry import OSEMParams
+
+        y_h = torch.empty(nb, dtype=torch.float32, pin_memory=True)
+        y_h.copy_(y)
+        sens_h = torch.empty(sens.shape, dtype=torch.float32, pin_memory=True)
+        sens_h.copy_(sens)
+        img_h = torch.empty(w.vol.shape_zyx, dtype=torch.float32, pin_memory=True)
+        img_h.copy_(img)
+        e2e_steps = 0
+        for s in range(nsub):
+            e2e_steps += s_fwd[s] + s_bwd(s)
+        prm1 = OSEMParams(n_iterations=1, n_subsets=nsub, convolution_interval=prm.convolution_interval,
+                          fwhm_xyz=list(prm.fwhm_xyz), cut_radius=prm.cut_radius)
+        ctx.osem(w.proj, y_h, w.vol, img_h, sens_h, prm1)  # stage buffers once (warm)
+        img_h.copy_(img)
+        t0 = time.perf_counter()
+        ctx.osem(w.proj, y_h, w.vol, img_h, sens_h, prm1)
+        dt = time.perf_counter() - t0
+        h2d = (nb + sens.numel() + nvox) * 4
+        result["e2e"] = {
+            "value": e2e_steps / dt,
+            "unit": UNIT,
+            "h2d_bytes_per_step": h2d // nsub,
+            "d2h_bytes_per_step": (nvox * 4) // nsub,
+            "call": "fir_osem with pinned host buffers, 1 iteration = "
+                    f"{nsub} steps, copies inside the timed region",
+            "osem_s_per_iteration": dt,
+        }
+
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        try:
+            r = cpu_reference_run(w, nsub)
+            result["cpu_baseline"] = {k2: r[k2] for k2 in ("value", "unit", "cores", "kind", "sample")}
+            result["cpu_baseline"]["osem_s_per_iteration"] = r["osem_s_per_iteration"]
+        except Exception as e:  # noqa: BLE001
+            result["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                                      "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        print(json.dumps(result))
+    ctx.close()
+    aux.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,1440 @@
+// C ABI of the B200 path (include/fir_cuda.h): validation, contexts, host
+// staging, geometry tables and launch orchestration.  Kernels live in
+// projector.cu and image_ops.cu.
+//
+// Validation reproduces the checks FIR performs before it projects, with
+// FIR's messages:
+//   ProjHeader::check             src_lib/ProjHeader.cc:6-106
+//   ProjGeometry::fill            src_lib/ProjHeader.cc:108-186
+//   ScannerHeader::check          src_lib/ScannerHeader.cc:26-303
+//   ScannerGeometry::fill         src_lib/ScannerHeader.cc:305-342
+//   VolHeader::check              src_lib/VolHeader.cc:5-29
+//   ScannerData::checkProjData    src_lib/ScannerData.cc:31-44
+//   ProjData::checkNSubsets       src_lib/ProjData.cc:166-174
+//   VolData::checkNFrames         src_lib/VolData.cc:227-233
+#include "../../include/fir_cuda.h"
+#include "internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace
+{
+using namespace fir;
+
+thread_local std::string g_error;
+
+struct Failure
+{
+  fir_status status;
+  std::string message;
+};
+
+template<typename... Args>
+[[noreturn]] void fail(fir_status s, Args&&... args)
+{
+  std::ostringstream os;
+  (os << ... << args);
+  throw Failure{s, os.str()};
+}
+
+void cuda_ok(cudaError_t e, const char* what)
+{
+  if (e != cudaSuccess)
+  {
+    cudaGetLastError();
+    if (e == cudaErrorMemoryAllocation)
+    {
+      fail(FIR_ERR_OUT_OF_MEMORY, what, ": ", cudaGetErrorString(e));
+    }
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+    {
+      fail(FIR_ERR_NO_DEVICE, what, ": ", cudaGetErrorString(e));
+    }
+    fail(FIR_ERR_CUDA, what, ": ", cudaGetErrorString(e));
+  }
+}
+
+template<typename F>
+fir_status guarded(F&& f)
+{
+  try
+  {
+    f();
+    return FIR_OK;
+  }
+  catch (const Failure& x)
+  {
+    g_error = x.message;
+    return x.status;
+  }
+  catch (const std::bad_alloc&)
+  {
+    g_error = "host allocation failed";
+    return FIR_ERR_OUT_OF_MEMORY;
+  }
+  catch (const std::exception& x)
+  {
+    g_error = x.what();
+    return FIR_ERR_INVALID_ARGUMENT;
+  }
+}
+
+// ------------------------------------------------------------ geometry
+
+struct ProjInfo
+{
+  fir_proj_desc d;
+  fir_proj_info g;
+  std::vector<int> n_axial;
+};
+
+ProjInfo check_proj(const fir_proj_desc* desc)
+{
+  if (desc == nullptr)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "projection descriptor is NULL");
+  }
+  ProjInfo p;
+  p.d = *desc;
+  auto& h = p.d;
+  if (h.n_rings <= 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "\"number of rings\" must be provided and > 0");
+  }
+  if (h.n_crystals_per_ring <= 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "\"number of crystals per ring\" must be provided and > 0");
+  }
+  if (h.n_crystals_per_ring % 4 != 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "\"number of crystals per ring\" must be a multiple of four");
+  }
+  if (h.segment_span <= 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "\"segment span\" must be > 0");
+  }
+  if (h.segment_span % 2 != 1)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "\"segment span\" must be an odd number");
+  }
+  const int max_span = 2 * h.n_rings - 1;
+  if (h.segment_span > max_span)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "For ", h.n_rings, " ring(s), \"segment span\" must not be > ", max_span);
+  }
+  if (h.n_segments < 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "\"number of segments\" must not be negative");
+  }
+  if (h.n_segments % 2 != 1)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "\"number of segments\" must be an odd number");
+  }
+  int max_nseg = max_span / h.segment_span;
+  max_nseg -= 1 - max_nseg % 2;
+  if (h.n_segments > max_nseg)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "For ", h.n_rings, " ring(s) and a segment span of ", h.segment_span,
+         ", \"number of segments\" must not be > ", max_nseg);
+  }
+  if (h.n_tang_coords < 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "\"number of tangential coordinates\" must not be negative");
+  }
+  const int max_tang = h.n_crystals_per_ring - 1;
+  if (h.n_tang_coords == 0)
+  {
+    h.n_tang_coords = max_tang;
+  }
+  else if (h.n_tang_coords > max_tang)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "For ", h.n_crystals_per_ring,
+         " crystals per ring, \"number of tangential coordinates\" must not be > ", max_tang);
+  }
+  if (h.n_segments > kMaxSegments)
+  {
+    fail(FIR_ERR_NOT_SUPPORTED, "at most ", kMaxSegments, " segments are supported");
+  }
+  // ProjGeometry::fill
+  auto& g = p.g;
+  g.seg_offset = (h.n_segments - 1) / 2;
+  g.tang_offset = h.n_tang_coords / 2;
+  g.n_tang_coords = h.n_tang_coords;
+  p.n_axial.resize(h.n_segments);
+  for (int seg = -g.seg_offset; seg <= g.seg_offset; ++seg)
+  {
+    const int a = seg < 0 ? -seg : seg;
+    int len;
+    if (h.segment_span == 1)
+    {
+      len = h.n_rings - a;
+    }
+    else
+    {
+      len = 2 * h.n_rings - 1;
+      if (a >= 1)
+      {
+        len -= h.segment_span + 1;
+      }
+      if (a >= 2)
+      {
+        len -= 2 * h.segment_span * (a - 1);
+      }
+    }
+    p.n_axial[seg + g.seg_offset] = len;
+  }
+  g.n_views = h.n_crystals_per_ring / 2;
+  g.n_bins = 0;
+  for (int len : p.n_axial)
+  {
+    g.n_bins += (long long)len * g.n_views * h.n_tang_coords;
+  }
+  g.half_span = (h.segment_span - 1) / 2;
+  g.max_ring_diff = h.segment_span == 1 ? g.seg_offset
+                                         : g.half_span + (g.seg_offset > 0 ? g.seg_offset * h.segment_span : 0);
+  if (g.n_bins > 0x7fffffffLL)
+  {
+    // FIR counts bins in int (ProjHeader.h:45)
+    fail(FIR_ERR_NOT_SUPPORTED, "total number of bins ", g.n_bins, " exceeds 2^31-1");
+  }
+  return p;
+}
+
+struct ScannerInfo
+{
+  int n_rings = 0, n_cpr = 0;
+  std::vector<double> xy, z;
+};
+
+ScannerInfo scanner_tables(const fir_scanner_desc* d0, bool tables)
+{
+  if (d0 == nullptr)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "scanner descriptor is NULL");
+  }
+  fir_scanner_desc s = *d0;
+  for (int i = 0; i < 3; ++i)
+  {
+    if (s.crystal_dims[i] < 0)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "Elements of \"crystal dimensions XYZ in mm\" must not be negative");
+    }
+  }
+  if (s.crystal_repeat[0] <= 0 || s.crystal_repeat[1] <= 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "Elements of \"crystal repeat numbers YZ\" must be > 0");
+  }
+  if (s.inter_crystal[0] < 0 || s.inter_crystal[1] < 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "Elements of \"inter-crystal distance YZ in mm\" must not be negative");
+  }
+  for (int i = 0; i < 3; ++i)
+  {
+    if (s.module_dims[i] < 0)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "Elements of \"module dimensions XYZ in mm\" must not be negative");
+    }
+  }
+  if (s.module_repeat[0] <= 0 || s.module_repeat[1] <= 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "Elements of \"module repeat numbers YZ\" must be > 0");
+  }
+  if (s.inter_module[0] < 0 || s.inter_module[1] < 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "Elements of \"inter-module distance YZ in mm\" must not be negative");
+  }
+  for (int i = 0; i < 3; ++i)
+  {
+    if (s.rsector_dims[i] < 0)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "Elements of \"rSector dimensions XYZ in mm\" must not be negative");
+    }
+  }
+  if (s.rsector_repeat <= 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "\"rSector repeat number\" must be present and > 0");
+  }
+  if (s.rsector_inner_radius <= 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "\"rSector inner radius in mm\" must be present and > 0");
+  }
+  if (s.crystal_repeat[0] > 1 && s.crystal_dims[1] == 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "Crystal repeat number in Y cannot be > 1 if crystal dimension in Y is zero");
+  }
+  if (s.crystal_repeat[1] > 1 && s.crystal_dims[2] == 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "Crystal repeat number in Z cannot be > 1 if crystal dimension in Z is zero");
+  }
+  const double min_mod[3] = {
+    s.crystal_dims[0],
+    s.crystal_dims[1] * s.crystal_repeat[0] + s.inter_crystal[0] * (s.crystal_repeat[0] - 1),
+    s.crystal_dims[2] * s.crystal_repeat[1] + s.inter_crystal[1] * (s.crystal_repeat[1] - 1)};
+  const char* axis = "XYZ";
+  for (int i = 0; i < 3; ++i)
+  {
+    if (s.module_dims[i] == 0.0)
+    {
+      s.module_dims[i] = min_mod[i];
+    }
+    else if (s.module_dims[i] < min_mod[i])
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "Module dimension in ", axis[i], " must be >= ", min_mod[i]);
+    }
+  }
+  if (s.module_repeat[0] > 1 && s.module_dims[1] == 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "Module repeat number in Y cannot be > 1 if module dimension in Y is zero");
+  }
+  if (s.module_repeat[1] > 1 && s.module_dims[2] == 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "Module repeat number in Z cannot be > 1 if module dimension in Z is zero");
+  }
+  const double min_rs[3] = {
+    s.module_dims[0],
+    s.module_dims[1] * s.module_repeat[0] + s.inter_module[0] * (s.module_repeat[0] - 1),
+    s.module_dims[2] * s.module_repeat[1] + s.inter_module[1] * (s.module_repeat[1] - 1)};
+  for (int i = 0; i < 3; ++i)
+  {
+    if (s.rsector_dims[i] == 0)
+    {
+      s.rsector_dims[i] = min_rs[i];
+    }
+    else if (s.rsector_dims[i] < min_rs[i])
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "rSector dimension in ", axis[i], " must be >= ", min_rs[i]);
+    }
+  }
+  ScannerInfo out;
+  out.n_cpr = s.crystal_repeat[0] * s.module_repeat[0] * s.rsector_repeat;
+  out.n_rings = s.crystal_repeat[1] * s.module_repeat[1];
+  if (!tables)
+  {
+    return out;
+  }
+  // ScannerData::computeCrystalXYPositionVector (ScannerData.cc:248-329):
+  // the first rSector is vertical at x = inner radius + depth/2 and is
+  // repeated by rotation; crystal 0 is the middle crystal of rSector 0.
+  const double cvy = s.crystal_dims[1] + s.inter_crystal[0];
+  const double cvz = s.crystal_dims[2] + s.inter_crystal[1];
+  const double mvy = s.module_dims[1] + s.inter_module[0];
+  const double mvz = s.module_dims[2] + s.inter_module[1];
+  const double tx = s.rsector_inner_radius + s.rsector_dims[0] / 2;
+  const int crystal_offset = s.module_repeat[0] * s.crystal_repeat[0] / 2;
+  const int ncy = s.crystal_repeat[0], nmy = s.module_repeat[0];
+  const double first_y = -((nmy - 1) * mvy + (ncy - 1) * cvy) / 2.0;
+  const int nrs = nmy * ncy;
+  std::vector<double> rsy(nrs);
+  for (int m = 0; m < nmy; ++m)
+  {
+    for (int c = 0; c < ncy; ++c)
+    {
+      rsy[m * ncy + c] = m * mvy + c * cvy + first_y;
+    }
+  }
+  const double angle_interval = 2 * 3.141592653589793 / s.rsector_repeat;
+  const int first_index = out.n_cpr - crystal_offset;
+  out.xy.resize(2 * (size_t)out.n_cpr);
+  for (int i = 0; i < first_index; ++i)
+  {
+    const double x = tx;
+    const int io = i + crystal_offset;
+    const double y = rsy[io % nrs];
+    const double angle = (io / nrs) * angle_interval;
+    const double ca = std::cos(angle);
+    const double sa = std::sin(angle);
+    out.xy[2 * i] = x * ca - y * sa;
+    out.xy[2 * i + 1] = x * sa + y * ca;
+  }
+  for (int i = first_index; i < out.n_cpr; ++i)
+  {
+    out.xy[2 * i] = tx;
+    out.xy[2 * i + 1] = rsy[i - first_index];
+  }
+  // computeSliceZPositionVector (ScannerData.cc:331-377): even slices on the
+  // rings, odd slices half-way between neighbouring rings.
+  const int ncz = s.crystal_repeat[1], nmz = s.module_repeat[1];
+  const double first_z = -((nmz - 1) * mvz + (ncz - 1) * cvz) / 2.0;
+  std::vector<double> ringz(nmz * ncz);
+  for (int m = 0; m < nmz; ++m)
+  {
+    for (int c = 0; c < ncz; ++c)
+    {
+      ringz[m * ncz + c] = m * mvz + c * cvz + first_z;
+    }
+  }
+  out.z.resize(2 * (size_t)out.n_rings - 1);
+  for (int k = 0; k < 2 * out.n_rings - 1; ++k)
+  {
+    out.z[k] = k % 2 == 0 ? ringz[k / 2] : (ringz[k / 2] + ringz[(k + 1) / 2]) / 2.0;
+  }
+  return out;
+}
+
+struct VolInfo
+{
+  fir_vol_desc d;
+  long long nvox;  // per frame
+};
+
+VolInfo check_vol(const fir_vol_desc* v)
+{
+  if (v == nullptr)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "volume descriptor is NULL");
+  }
+  if (v->nx <= 0 || v->ny <= 0 || v->nz <= 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "Number of voxels must be greater than zero in each dimension");
+  }
+  if (!(v->voxel_x > 0) || !(v->voxel_y > 0) || !(v->voxel_z > 0))
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "Voxel extent must be greater than zero in each dimension");
+  }
+  if (v->n_frames <= 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "Number of frames must be greater than zero");
+  }
+  VolInfo out{*v, (long long)v->nx * v->ny * v->nz};
+  if (out.nvox > 0x7fffffffLL)
+  {
+    // FIR indexes voxels with int (types.h:7-8)
+    fail(FIR_ERR_NOT_SUPPORTED, "volume of ", out.nvox, " voxels exceeds 2^31-1");
+  }
+  return out;
+}
+
+void check_frames(const VolInfo& v, int n)
+{
+  if (v.d.n_frames != n)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "Wrong number of frames (expected ", n, ")");
+  }
+}
+
+void check_subsets(const ProjInfo& p, int n_subsets)
+{
+  if (n_subsets <= 0 || p.g.n_views % n_subsets != 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "Number of subsets must be a divisor of ", p.g.n_views);
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ context
+
+struct DevBuf
+{
+  void* p = nullptr;
+  size_t bytes = 0;
+
+  void* ensure(size_t n)
+  {
+    if (n > bytes)
+    {
+      if (p != nullptr)
+      {
+        cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+      }
+      cuda_ok(cudaMalloc(&p, n), "cudaMalloc");
+      bytes = n;
+    }
+    return p;
+  }
+
+  void release()
+  {
+    if (p != nullptr)
+    {
+      cudaFree(p);
+    }
+    p = nullptr;
+    bytes = 0;
+  }
+};
+
+struct fir_ctx
+{
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int geometry = FIR_GEOMETRY_REFERENCE;
+  int backproj = FIR_BACKPROJ_ATOMIC;
+  int skip_zero = 0;
+  int block = 128;
+  long long launches = 0;
+
+  bool have_scanner = false;
+  int scan_rings = 0, scan_cpr = 0;
+  DevBuf xy, z;
+
+  DevBuf check;     // device check word
+  int* check_host = nullptr;  // pinned mirror
+
+  DevBuf bp, conv1, conv2, conv_copy, mu;
+  std::vector<DevBuf> staging;
+
+  // projector-kernel timing (FIR_OPT_TIMING)
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending;
+  double timed_ms = 0.0;
+  long long timed_n = 0;
+};
+
+namespace
+{
+fir_ctx& check_ctx(fir_ctx* c)
+{
+  if (c == nullptr)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "context is NULL");
+  }
+  cuda_ok(cudaSetDevice(c->device), "cudaSetDevice");
+  return *c;
+}
+
+LaunchCfg cfg_of(fir_ctx& c)
+{
+  return LaunchCfg{c.block, c.stream, static_cast<int*>(c.check.p)};
+}
+
+void after_launch(fir_ctx& c, int n = 1)
+{
+  c.launches += n;
+  cuda_ok(cudaGetLastError(), "kernel launch");
+}
+
+cudaEvent_t take_event(fir_ctx& c)
+{
+  if (!c.ev_pool.empty())
+  {
+    cudaEvent_t e = c.ev_pool.back();
+    c.ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cuda_ok(cudaEventCreate(&e), "cudaEventCreate");
+  return e;
+}
+
+// Brackets one projector-kernel launch with events when timing is on.
+template<typename F>
+void timed_launch(fir_ctx& c, F&& launch)
+{
+  if (!c.timing)
+  {
+    launch();
+    after_launch(c);
+    return;
+  }
+  cudaEvent_t a = take_event(c), b = take_event(c);
+  cuda_ok(cudaEventRecord(a, c.stream), "cudaEventRecord");
+  launch();
+  after_launch(c);
+  cuda_ok(cudaEventRecord(b, c.stream), "cudaEventRecord");
+  c.ev_pending.emplace_back(a, b);
+}
+
+void drain_timing(fir_ctx& c)
+{
+  for (auto& p : c.ev_pending)
+  {
+    cuda_ok(cudaEventSynchronize(p.second), "cudaEventSynchronize");
+    float ms = 0.0f;
+    cuda_ok(cudaEventElapsedTime(&ms, p.first, p.second), "cudaEventElapsedTime");
+    c.timed_ms += ms;
+    c.timed_n += 1;
+    c.ev_pool.push_back(p.first);
+    c.ev_pool.push_back(p.second);
+  }
+  c.ev_pending.clear();
+}
+
+Tables tables_of(fir_ctx& c, const ProjInfo& p)
+{
+  if (!c.have_scanner)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "no scanner set on the context (fir_ctx_set_scanner)");
+  }
+  if (p.d.n_rings != c.scan_rings || p.d.n_crystals_per_ring != c.scan_cpr)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "Projection must have the same number of rings (", c.scan_rings,
+         ") and the same number of crystals per ring (", c.scan_cpr, ") as the scanner");
+  }
+  return Tables{static_cast<const double2*>(c.xy.p), static_cast<const double*>(c.z.p)};
+}
+
+Grid grid_of(const fir_ctx& c, const VolInfo& v)
+{
+  const double vox[3] = {v.d.voxel_x, v.d.voxel_y, v.d.voxel_z};
+  Grid g;
+  g.nx = v.d.nx;
+  g.ny = v.d.ny;
+  g.nz = v.d.nz;
+  g.nxy = v.d.nx * v.d.ny;
+  for (int d = 0; d < 3; ++d)
+  {
+    if (c.geometry == FIR_GEOMETRY_REFERENCE)
+    {
+      // Siddon.h:113 keeps the voxel extents as int
+      g.ext[d] = (double)(int)vox[d];
+      if (g.ext[d] <= 0.0)
+      {
+        fail(FIR_ERR_INVALID_ARGUMENT, "voxel extent ", vox[d],
+             " mm truncates to 0 in FIR's traversal (use FIR_GEOMETRY_EXACT)");
+      }
+    }
+    else
+    {
+      g.ext[d] = vox[d];
+    }
+  }
+  const double depth = v.d.nz * v.d.voxel_z;
+  g.low[0] = v.d.offset_x - v.d.voxel_x / 2;
+  g.low[1] = v.d.offset_y - v.d.voxel_y / 2;
+  g.low[2] = v.d.offset_z - depth / 2;
+  g.high[0] = g.low[0] + v.d.nx * v.d.voxel_x;
+  g.high[1] = g.low[1] + v.d.ny * v.d.voxel_y;
+  g.high[2] = g.low[2] + depth;
+  return g;
+}
+
+Sino sino_of(const ProjInfo& p, int n_subsets, int subset)
+{
+  Sino s;
+  std::memset(&s, 0, sizeof(s));
+  s.n_rings = p.d.n_rings;
+  s.n_cpr = p.d.n_crystals_per_ring;
+  s.span = p.d.segment_span;
+  s.half_span = p.g.half_span;
+  s.n_segments = p.d.n_segments;
+  s.seg_offset = p.g.seg_offset;
+  s.tang_offset = p.g.tang_offset;
+  s.n_views = p.g.n_views;
+  s.n_tang = p.g.n_tang_coords;
+  s.n_subsets = n_subsets;
+  s.subset = subset;
+  long long base = 0;
+  for (int k = 0; k < s.n_segments; ++k)
+  {
+    s.seg_base[k] = (int)base;
+    s.enum_base[k] = (int)(base / n_subsets);
+    s.n_axial[k] = p.n_axial[k];
+    base += (long long)p.n_axial[k] * s.n_views * s.n_tang;
+  }
+  s.seg_base[s.n_segments] = (int)base;
+  s.enum_base[s.n_segments] = (int)(base / n_subsets);
+  s.n_enum = (int)(base / n_subsets);
+  return s;
+}
+
+bool is_device_ptr(const void* p)
+{
+  if (p == nullptr)
+  {
+    return false;
+  }
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess)
+  {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Gives device views of caller buffers.  Device pointers pass through; host
+// pointers are copied into context-owned device buffers (in), and copied
+// back when finish() runs (out).  A call with any host pointer is
+// synchronous: finish() waits for the stream and reports device checks.
+class Stager
+{
+public:
+  explicit Stager(fir_ctx& c): c_(c) {}
+
+  template<typename T>
+  const T* in(const T* p, long long n)
+  {
+    return static_cast<const T*>(stage(const_cast<T*>(p), n * (long long)sizeof(T), true, false));
+  }
+
+  template<typename T>
+  T* out(T* p, long long n)
+  {
+    return static_cast<T*>(stage(p, n * (long long)sizeof(T), false, true));
+  }
+
+  template<typename T>
+  T* inout(T* p, long long n)
+  {
+    return static_cast<T*>(stage(p, n * (long long)sizeof(T), true, true));
+  }
+
+  bool host() const { return any_host_; }
+
+  void finish()
+  {
+    for (auto& b : back_)
+    {
+      cuda_ok(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, c_.stream), "cudaMemcpyAsync D2H");
+    }
+    if (any_host_)
+    {
+      cuda_ok(cudaStreamSynchronize(c_.stream), "cudaStreamSynchronize");
+    }
+  }
+
+private:
+  struct Back
+  {
+    void* host;
+    void* dev;
+    size_t bytes;
+  };
+
+  void* stage(void* p, long long bytes, bool copy_in, bool copy_out)
+  {
+    if (p == nullptr || is_device_ptr(p))
+    {
+      return p;
+    }
+    any_host_ = true;
+    if (slot_ >= c_.staging.size())
+    {
+      c_.staging.resize(slot_ + 1);
+    }
+    void* d = c_.staging[slot_++].ensure((size_t)std::max<long long>(bytes, 16));
+    if (copy_in)
+    {
+      cuda_ok(cudaMemcpyAsync(d, p, (size_t)bytes, cudaMemcpyHostToDevice, c_.stream), "cudaMemcpyAsync H2D");
+    }
+    if (copy_out)
+    {
+      back_.push_back(Back{p, d, (size_t)bytes});
+    }
+    return d;
+  }
+
+  fir_ctx& c_;
+  size_t slot_ = 0;
+  bool any_host_ = false;
+  std::vector<Back> back_;
+};
+
+void read_checks(fir_ctx& c)
+{
+  cuda_ok(cudaMemcpyAsync(c.check_host, c.check.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream),
+          "cudaMemcpyAsync check word");
+  cuda_ok(cudaStreamSynchronize(c.stream), "cudaStreamSynchronize");
+  const int word = *c.check_host;
+  if (word != 0)
+  {
+    cuda_ok(cudaMemsetAsync(c.check.p, 0, sizeof(int), c.stream), "cudaMemsetAsync");
+    if (word & kCheckWalkGuard)
+    {
+      fail(FIR_ERR_DEVICE_CHECK, "a Siddon traversal exceeded its iteration bound (non-finite coordinates?)");
+    }
+    fail(FIR_ERR_DEVICE_CHECK, "device check word ", word);
+  }
+}
+
+void finish(fir_ctx& c, Stager& st)
+{
+  st.finish();
+  if (st.host())
+  {
+    read_checks(c);
+  }
+}
+
+Taps gauss_taps(float fwhm, double vox, bool double_sigma)
+{
+  // operations.cc:32-75: half width (int(6 sigma / voxel) + 1) / 2, weights
+  // exp(-k^2 voxel^2 / (2 sigma^2)).  sigma is float for x and y (divisor
+  // 2.3548f) and double for z (divisor 2.3548).
+  Taps t;
+  std::memset(&t, 0, sizeof(t));
+  if (double_sigma)
+  {
+    const double sigma = fwhm / 2.3548;
+    t.half = (static_cast<int>(6.0 * sigma / vox) + 1) / 2;
+    if (t.half > kMaxHalfTaps)
+    {
+      fail(FIR_ERR_NOT_SUPPORTED, "Gaussian filter half width ", t.half, " exceeds ", kMaxHalfTaps);
+    }
+    for (int k = -t.half; k <= t.half; ++k)
+    {
+      t.w[t.half + k] = (float)std::exp(-(k * k * vox * vox) / (2 * sigma * sigma));
+    }
+  }
+  else
+  {
+    const float sigma = fwhm / 2.3548f;
+    t.half = (static_cast<int>(6.0 * sigma / vox) + 1) / 2;
+    if (t.half > kMaxHalfTaps)
+    {
+      fail(FIR_ERR_NOT_SUPPORTED, "Gaussian filter half width ", t.half, " exceeds ", kMaxHalfTaps);
+    }
+    for (int k = -t.half; k <= t.half; ++k)
+    {
+      t.w[t.half + k] = (float)std::exp(-(k * k * vox * vox) / (2 * sigma * sigma));
+    }
+  }
+  return t;
+}
+
+// operations::convolve on device memory, all frames of vol.
+void convolve_device(fir_ctx& c, const VolInfo& v, float* img, const float fwhm[3], float cut)
+{
+  if (!(fwhm[0] > 0.0 && fwhm[1] > 0.0 && fwhm[2] > 0.0))
+  {
+    return;
+  }
+  const Taps tx = gauss_taps(fwhm[0], v.d.voxel_x, false);
+  const Taps ty = gauss_taps(fwhm[1], v.d.voxel_y, false);
+  const Taps tz = gauss_taps(fwhm[2], v.d.voxel_z, true);
+  const size_t bytes = (size_t)v.nvox * sizeof(float);
+  float* t1 = static_cast<float*>(c.conv1.ensure(bytes));
+  float* t2 = static_cast<float*>(c.conv2.ensure(bytes));
+  float* cp = cut > 0.0f ? static_cast<float*>(c.conv_copy.ensure(bytes)) : nullptr;
+  const LaunchCfg cfg = cfg_of(c);
+  const float f = fwhm[0] > fwhm[1] ? fwhm[0] : fwhm[1];
+  for (int fr = 0; fr < v.d.n_frames; ++fr)
+  {
+    float* x = img + (size_t)fr * v.nvox;
+    if (cp != nullptr)
+    {
+      cuda_ok(cudaMemcpyAsync(cp, x, bytes, cudaMemcpyDeviceToDevice, c.stream), "cudaMemcpyAsync");
+    }
+    launch_conv_pass(v.d.nx, v.d.ny, v.d.nz, 0, tx, x, t1, cfg);
+    launch_conv_pass(v.d.nx, v.d.ny, v.d.nz, 1, ty, t1, t2, cfg);
+    launch_conv_pass(v.d.nx, v.d.ny, v.d.nz, 2, tz, t2, x, cfg);
+    after_launch(c, 3);
+    if (cp != nullptr)
+    {
+      launch_conv_restore(v.d.nx, v.d.ny, v.d.nz, v.d.voxel_x, v.d.voxel_y, cut, f, cp, x, cfg);
+      after_launch(c);
+    }
+  }
+}
+
+void cut_device(fir_ctx& c, const VolInfo& v, float* img, float cut, int frames)
+{
+  if (!(cut > 0.0f))
+  {
+    return;
+  }
+  for (int fr = 0; fr < frames; ++fr)
+  {
+    launch_cut_circle(v.d.nx, v.d.ny, v.d.nz, v.d.voxel_x, v.d.voxel_y, cut, img + (size_t)fr * v.nvox,
+                      cfg_of(c));
+    after_launch(c);
+  }
+}
+
+void check_osem_params(const fir_osem_params* prm, const ProjInfo& p)
+{
+  if (prm == nullptr)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "OSEM parameters are NULL");
+  }
+  check_subsets(p, prm->n_subsets);
+  if (prm->n_iterations < 0)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "number of iterations must not be negative");
+  }
+}
+
+// Device-pointer body of one OSEM sub-iteration.
+void osem_subiteration_device(fir_ctx& c, const ProjInfo& p, const Tables& t, const Grid& g,
+                              const VolInfo& v, const float* sino, const float* bias, float* img,
+                              const float* sens_frame, const fir_osem_params* prm, int subset,
+                              int subiter)
+{
+  float* bp = static_cast<float*>(c.bp.ensure((size_t)v.nvox * sizeof(float)));
+  cuda_ok(cudaMemsetAsync(bp, 0, (size_t)v.nvox * sizeof(float), c.stream), "cudaMemsetAsync");
+  const Sino s = sino_of(p, prm->n_subsets, subset);
+  timed_launch(c, [&] { launch_osem_subset(g, s, t, img, sino, bias, bp, c.skip_zero != 0, cfg_of(c)); });
+  launch_em_update(v.nvox, img, bp, sens_frame, cfg_of(c));
+  after_launch(c);
+  const bool conv = prm->convolution_interval > 0 && prm->fwhm_xyz[0] > 0.0 && prm->fwhm_xyz[1] > 0.0 &&
+                    prm->fwhm_xyz[2] > 0.0;
+  if (conv && subiter % prm->convolution_interval == 0)
+  {
+    convolve_device(c, v, img, prm->fwhm_xyz, prm->cut_radius);
+  }
+  cut_device(c, v, img, prm->cut_radius, 1);
+}
+
+}  // namespace
+
+// ================================================================== ABI
+
+extern "C" {
+
+int fir_abi_version(void) { return FIR_CUDA_ABI_VERSION; }
+
+const char* fir_last_error(void) { return g_error.c_str(); }
+
+const char* fir_status_string(fir_status s)
+{
+  switch (s)
+  {
+  case FIR_OK: return "FIR_OK";
+  case FIR_ERR_INVALID_ARGUMENT: return "FIR_ERR_INVALID_ARGUMENT";
+  case FIR_ERR_CUDA: return "FIR_ERR_CUDA";
+  case FIR_ERR_OUT_OF_MEMORY: return "FIR_ERR_OUT_OF_MEMORY";
+  case FIR_ERR_DEVICE_CHECK: return "FIR_ERR_DEVICE_CHECK";
+  case FIR_ERR_NO_DEVICE: return "FIR_ERR_NO_DEVICE";
+  case FIR_ERR_NOT_SUPPORTED: return "FIR_ERR_NOT_SUPPORTED";
+  }
+  return "unknown fir_status";
+}
+
+fir_status fir_proj_geometry(const fir_proj_desc* desc, fir_proj_info* geom, int* n_axial)
+{
+  return guarded([&] {
+    const ProjInfo p = check_proj(desc);
+    if (geom != nullptr)
+    {
+      *geom = p.g;
+    }
+    if (n_axial != nullptr)
+    {
+      std::copy(p.n_axial.begin(), p.n_axial.end(), n_axial);
+    }
+  });
+}
+
+fir_status fir_scanner_tables(const fir_scanner_desc* desc, double* xy, double* z, int* n_rings,
+                              int* n_crystals_per_ring)
+{
+  return guarded([&] {
+    const ScannerInfo s = scanner_tables(desc, xy != nullptr || z != nullptr);
+    if (n_rings != nullptr)
+    {
+      *n_rings = s.n_rings;
+    }
+    if (n_crystals_per_ring != nullptr)
+    {
+      *n_crystals_per_ring = s.n_cpr;
+    }
+    if (xy != nullptr)
+    {
+      std::copy(s.xy.begin(), s.xy.end(), xy);
+    }
+    if (z != nullptr)
+    {
+      std::copy(s.z.begin(), s.z.end(), z);
+    }
+  });
+}
+
+fir_status fir_ctx_create(fir_ctx** out, int device)
+{
+  return guarded([&] {
+    if (out == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "output pointer is NULL");
+    }
+    *out = nullptr;
+    int n = 0;
+    cuda_ok(cudaGetDeviceCount(&n), "cudaGetDeviceCount");
+    if (device < 0 || device >= n)
+    {
+      fail(FIR_ERR_NO_DEVICE, "device ", device, " not present (", n, " visible)");
+    }
+    cuda_ok(cudaSetDevice(device), "cudaSetDevice");
+    auto* c = new fir_ctx();
+    c->device = device;
+    try
+    {
+      c->check.ensure(sizeof(int));
+      cuda_ok(cudaMemset(c->check.p, 0, sizeof(int)), "cudaMemset");
+      cuda_ok(cudaMallocHost(&c->check_host, sizeof(int)), "cudaMallocHost");
+    }
+    catch (...)
+    {
+      c->check.release();
+      delete c;
+      throw;
+    }
+    *out = c;
+  });
+}
+
+fir_status fir_ctx_destroy(fir_ctx* c)
+{
+  return guarded([&] {
+    if (c == nullptr)
+    {
+      return;
+    }
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (DevBuf* b : {&c->xy, &c->z, &c->check, &c->bp, &c->conv1, &c->conv2, &c->conv_copy, &c->mu})
+    {
+      b->release();
+    }
+    for (auto& b : c->staging)
+    {
+      b.release();
+    }
+    for (auto& p : c->ev_pending)
+    {
+      cudaEventDestroy(p.first);
+      cudaEventDestroy(p.second);
+    }
+    for (auto e : c->ev_pool)
+    {
+      cudaEventDestroy(e);
+    }
+    if (c->check_host != nullptr)
+    {
+      cudaFreeHost(c->check_host);
+    }
+    delete c;
+  });
+}
+
+fir_status fir_ctx_set_stream(fir_ctx* ctx, void* stream)
+{
+  return guarded([&] { check_ctx(ctx).stream = static_cast<cudaStream_t>(stream); });
+}
+
+fir_status fir_ctx_set_option(fir_ctx* ctx, fir_option opt, int value)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    switch (opt)
+    {
+    case FIR_OPT_GEOMETRY:
+      if (value != FIR_GEOMETRY_REFERENCE && value != FIR_GEOMETRY_EXACT)
+      {
+        fail(FIR_ERR_INVALID_ARGUMENT, "unknown geometry mode ", value);
+      }
+      c.geometry = value;
+      break;
+    case FIR_OPT_BACKPROJ_MODE:
+      if (value != FIR_BACKPROJ_ATOMIC && value != FIR_BACKPROJ_DETERMINISTIC)
+      {
+        fail(FIR_ERR_INVALID_ARGUMENT, "unknown backprojection mode ", value);
+      }
+      if (value == FIR_BACKPROJ_DETERMINISTIC)
+      {
+        fail(FIR_ERR_NOT_SUPPORTED, "deterministic backprojection is not available in this build");
+      }
+      c.backproj = value;
+      break;
+    case FIR_OPT_SKIP_ZERO_BINS:
+      c.skip_zero = value != 0;
+      break;
+    case FIR_OPT_BLOCK_SIZE:
+      if (value == 0)
+      {
+        value = 128;
+      }
+      if (value < 32 || value > 256 || value % 32 != 0)
+      {
+        fail(FIR_ERR_INVALID_ARGUMENT, "block size must be a multiple of 32 in [32, 256]");
+      }
+      c.block = value;
+      break;
+    case FIR_OPT_TIMING:
+      c.timing = value != 0;
+      break;
+    default:
+      fail(FIR_ERR_INVALID_ARGUMENT, "unknown option ", (int)opt);
+    }
+  });
+}
+
+fir_status fir_ctx_projector_time(fir_ctx* ctx, double* ms, long long* launches, int reset)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    drain_timing(c);
+    if (ms != nullptr)
+    {
+      *ms = c.timed_ms;
+    }
+    if (launches != nullptr)
+    {
+      *launches = c.timed_n;
+    }
+    if (reset)
+    {
+      c.timed_ms = 0.0;
+      c.timed_n = 0;
+    }
+  });
+}
+
+fir_status fir_ctx_get_option(fir_ctx* ctx, fir_option opt, int* value)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    if (value == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "output pointer is NULL");
+    }
+    switch (opt)
+    {
+    case FIR_OPT_GEOMETRY: *value = c.geometry; break;
+    case FIR_OPT_BACKPROJ_MODE: *value = c.backproj; break;
+    case FIR_OPT_SKIP_ZERO_BINS: *value = c.skip_zero; break;
+    case FIR_OPT_BLOCK_SIZE: *value = c.block; break;
+    case FIR_OPT_TIMING: *value = c.timing ? 1 : 0; break;
+    default: fail(FIR_ERR_INVALID_ARGUMENT, "unknown option ", (int)opt);
+    }
+  });
+}
+
+fir_status fir_ctx_set_scanner(fir_ctx* ctx, const fir_scanner_desc* scanner)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const ScannerInfo s = scanner_tables(scanner, true);
+    cuda_ok(cudaStreamSynchronize(c.stream), "cudaStreamSynchronize");
+    c.xy.ensure(s.xy.size() * sizeof(double));
+    c.z.ensure(s.z.size() * sizeof(double));
+    cuda_ok(cudaMemcpy(c.xy.p, s.xy.data(), s.xy.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
+    cuda_ok(cudaMemcpy(c.z.p, s.z.data(), s.z.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
+    c.scan_rings = s.n_rings;
+    c.scan_cpr = s.n_cpr;
+    c.have_scanner = true;
+  });
+}
+
+fir_status fir_ctx_synchronize(fir_ctx* ctx)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    read_checks(c);
+  });
+}
+
+long long fir_ctx_launch_count(const fir_ctx* ctx) { return ctx != nullptr ? ctx->launches : -1; }
+
+fir_status fir_forward(fir_ctx* ctx, const fir_vol_desc* vol, const float* img, const fir_proj_desc* proj,
+                       float* sino)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const VolInfo v = check_vol(vol);
+    const ProjInfo p = check_proj(proj);
+    const Tables t = tables_of(c, p);
+    const Grid g = grid_of(c, v);
+    Stager st(c);
+    const float* dimg = st.in(img, v.nvox);
+    float* dsino = st.out(sino, p.g.n_bins);
+    const Sino s = sino_of(p, 1, 0);
+    timed_launch(c, [&] { launch_forward(g, s, t, dimg, dsino, FwdEpilogue::None, cfg_of(c)); });
+    finish(c, st);
+  });
+}
+
+fir_status fir_forward_exp(fir_ctx* ctx, const fir_vol_desc* vol, const float* mu, const fir_proj_desc* proj,
+                           float* acf)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const VolInfo v = check_vol(vol);
+    const ProjInfo p = check_proj(proj);
+    const Tables t = tables_of(c, p);
+    const Grid g = grid_of(c, v);
+    Stager st(c);
+    const float* dmu = st.in(mu, v.nvox);
+    float* dacf = st.out(acf, p.g.n_bins);
+    const Sino s = sino_of(p, 1, 0);
+    timed_launch(c, [&] { launch_forward(g, s, t, dmu, dacf, FwdEpilogue::Exp, cfg_of(c)); });
+    finish(c, st);
+  });
+}
+
+fir_status fir_backward(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const fir_vol_desc* vol,
+                        float* img, int n_subsets)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const ProjInfo p = check_proj(proj);
+    check_subsets(p, n_subsets);
+    const VolInfo v = check_vol(vol);
+    check_frames(v, n_subsets);
+    const Tables t = tables_of(c, p);
+    const Grid g = grid_of(c, v);
+    if (sino == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "sinogram is NULL");
+    }
+    Stager st(c);
+    const float* dsino = st.in(sino, p.g.n_bins);
+    float* dimg = st.out(img, v.nvox * n_subsets);
+    cuda_ok(cudaMemsetAsync(dimg, 0, (size_t)(v.nvox * n_subsets) * sizeof(float), c.stream), "cudaMemsetAsync");
+    for (int s = 0; s < n_subsets; ++s)
+    {
+      const Sino ss = sino_of(p, n_subsets, s);
+      timed_launch(c, [&] {
+        launch_backward(g, ss, t, dsino, dimg + (size_t)s * v.nvox, c.skip_zero != 0, cfg_of(c));
+      });
+    }
+    finish(c, st);
+  });
+}
+
+fir_status fir_sensitivity(fir_ctx* ctx, const fir_proj_desc* proj, const fir_vol_desc* vol, float* sens,
+                           int n_subsets)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const ProjInfo p = check_proj(proj);
+    check_subsets(p, n_subsets);
+    const VolInfo v = check_vol(vol);
+    check_frames(v, n_subsets);
+    const Tables t = tables_of(c, p);
+    const Grid g = grid_of(c, v);
+    Stager st(c);
+    float* dsens = st.out(sens, v.nvox * n_subsets);
+    cuda_ok(cudaMemsetAsync(dsens, 0, (size_t)(v.nvox * n_subsets) * sizeof(float), c.stream), "cudaMemsetAsync");
+    for (int s = 0; s < n_subsets; ++s)
+    {
+      const Sino ss = sino_of(p, n_subsets, s);
+      timed_launch(c, [&] { launch_backward(g, ss, t, nullptr, dsens + (size_t)s * v.nvox, false, cfg_of(c)); });
+    }
+    finish(c, st);
+  });
+}
+
+fir_status fir_osem_subiteration(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const float* bias,
+                                 const fir_vol_desc* vol, float* img, const float* sens_frame,
+                                 const fir_osem_params* params, int subset, int subiter)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const ProjInfo p = check_proj(proj);
+    check_osem_params(params, p);
+    if (subset < 0 || subset >= params->n_subsets)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "subset ", subset, " out of range [0, ", params->n_subsets, ")");
+    }
+    const VolInfo v = check_vol(vol);
+    check_frames(v, 1);
+    const Tables t = tables_of(c, p);
+    const Grid g = grid_of(c, v);
+    if (sino == nullptr || sens_frame == nullptr || img == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "sinogram, image and sensitivity must not be NULL");
+    }
+    Stager st(c);
+    const float* dsino = st.in(sino, p.g.n_bins);
+    const float* dbias = st.in(bias, p.g.n_bins);
+    const float* dsens = st.in(sens_frame, v.nvox);
+    float* dimg = st.inout(img, v.nvox);
+    osem_subiteration_device(c, p, t, g, v, dsino, dbias, dimg, dsens, params, subset, subiter);
+    finish(c, st);
+  });
+}
+
+fir_status fir_osem(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const float* bias,
+                    const fir_vol_desc* vol, float* img, const float* sens, const fir_osem_params* params,
+                    fir_osem_save_fn save, void* user)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const ProjInfo p = check_proj(proj);
+    check_osem_params(params, p);
+    const VolInfo v = check_vol(vol);
+    check_frames(v, 1);
+    const Tables t = tables_of(c, p);
+    const Grid g = grid_of(c, v);
+    if (sino == nullptr || sens == nullptr || img == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "sinogram, image and sensitivity must not be NULL");
+    }
+    Stager st(c);
+    const float* dsino = st.in(sino, p.g.n_bins);
+    const float* dbias = st.in(bias, p.g.n_bins);
+    const float* dsens = st.in(sens, v.nvox * params->n_subsets);
+    float* dimg = st.inout(img, v.nvox);
+    std::vector<float> host_copy;
+    cut_device(c, v, dimg, params->cut_radius, 1);
+    const int nsub_total = params->n_iterations * params->n_subsets;
+    for (int iter = 0; iter < params->n_iterations; ++iter)
+    {
+      for (int subset = 0; subset < params->n_subsets; ++subset)
+      {
+        const int subiter = iter * params->n_subsets + subset + 1;
+        osem_subiteration_device(c, p, t, g, v, dsino, dbias, dimg, dsens + (size_t)subset * v.nvox, params,
+                                 subset, subiter);
+        if (save != nullptr && params->save_interval > 0 && subiter % params->save_interval == 0 &&
+            subiter != nsub_total)
+        {
+          host_copy.resize((size_t)v.nvox);
+          cuda_ok(cudaMemcpyAsync(host_copy.data(), dimg, (size_t)v.nvox * sizeof(float), cudaMemcpyDeviceToHost,
+                                  c.stream),
+                  "cudaMemcpyAsync");
+          cuda_ok(cudaStreamSynchronize(c.stream), "cudaStreamSynchronize");
+          save(user, subiter, host_copy.data());
+        }
+      }
+    }
+    finish(c, st);
+  });
+}
+
+fir_status fir_em_update(fir_ctx* ctx, const fir_vol_desc* vol, float* img, float* bp, const float* sens_frame)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const VolInfo v = check_vol(vol);
+    Stager st(c);
+    float* dimg = st.inout(img, v.nvox);
+    float* dbp = st.inout(bp, v.nvox);
+    const float* dsens = st.in(sens_frame, v.nvox);
+    launch_em_update(v.nvox, dimg, dbp, dsens, cfg_of(c));
+    after_launch(c);
+    finish(c, st);
+  });
+}
+
+fir_status fir_convolve(fir_ctx* ctx, const fir_vol_desc* vol, float* img, const float fwhm_xyz[3],
+                        float cut_radius)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const VolInfo v = check_vol(vol);
+    if (fwhm_xyz == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "fwhm is NULL");
+    }
+    Stager st(c);
+    float* dimg = st.inout(img, v.nvox * v.d.n_frames);
+    convolve_device(c, v, dimg, fwhm_xyz, cut_radius);
+    finish(c, st);
+  });
+}
+
+fir_status fir_cut_circle(fir_ctx* ctx, const fir_vol_desc* vol, float* img, float cut_radius)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const VolInfo v = check_vol(vol);
+    Stager st(c);
+    float* dimg = st.inout(img, v.nvox);
+    cut_device(c, v, dimg, cut_radius, 1);
+    finish(c, st);
+  });
+}
+
+fir_status fir_apply_mask(fir_ctx* ctx, const fir_vol_desc* vol, float* img, const float* mask)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const VolInfo v = check_vol(vol);
+    Stager st(c);
+    float* dimg = st.inout(img, v.nvox);
+    const float* dmask = st.in(mask, v.nvox);
+    launch_apply_mask(v.nvox, dimg, dmask, cfg_of(c));
+    after_launch(c);
+    finish(c, st);
+  });
+}
+
+fir_status fir_hu_to_mu(fir_ctx* ctx, const fir_vol_desc* vol, float* img)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const VolInfo v = check_vol(vol);
+    Stager st(c);
+    float* dimg = st.inout(img, v.nvox);
+    launch_hu_to_mu(v.nvox, dimg, cfg_of(c));
+    after_launch(c);
+    finish(c, st);
+  });
+}
+
+fir_status fir_proj_exponential(fir_ctx* ctx, const fir_proj_desc* proj, float* sino)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const ProjInfo p = check_proj(proj);
+    Stager st(c);
+    float* d = st.inout(sino, p.g.n_bins);
+    launch_exponential(p.g.n_bins, d, cfg_of(c));
+    after_launch(c);
+    finish(c, st);
+  });
+}
+
+fir_status fir_proj_multiply(fir_ctx* ctx, const fir_proj_desc* proj, float* a, const float* b)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const ProjInfo p = check_proj(proj);
+    Stager st(c);
+    float* da = st.inout(a, p.g.n_bins);
+    const float* db = st.in(b, p.g.n_bins);
+    launch_proj_multiply(p.g.n_bins, da, db, cfg_of(c));
+    after_launch(c);
+    finish(c, st);
+  });
+}
+
+fir_status fir_siddon_paths(fir_ctx* ctx, const fir_vol_desc* vol, long long n, const double* ends, int cap,
+                            int* coords, double* lengths, int* counts, int* crosses)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const VolInfo v = check_vol(vol);
+    const Grid g = grid_of(c, v);
+    if (n < 0 || cap < 0)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "negative count");
+    }
+    Stager st(c);
+    const double* de = st.in(ends, 6 * n);
+    int* dco = st.out(coords, n * cap);
+    double* dle = st.out(lengths, n * cap);
+    int* dcn = st.out(counts, n);
+    int* dcr = st.out(crosses, n);
+    launch_siddon_paths(g, n, de, cap, dco, dle, dcn, dcr, cfg_of(c));
+    after_launch(c);
+    finish(c, st);
+  });
+}
+
+fir_status fir_lor_paths(fir_ctx* ctx, const fir_proj_desc* proj, const fir_vol_desc* vol, long long n,
+                         const long long* bins, int cap, int* coords, double* lengths, int* counts, int* crosses)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const ProjInfo p = check_proj(proj);
+    const VolInfo v = check_vol(vol);
+    const Tables t = tables_of(c, p);
+    const Grid g = grid_of(c, v);
+    if (n < 0 || cap < 0)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "negative count");
+    }
+    Stager st(c);
+    const long long* db = st.in(bins, n);
+    int* dco = st.out(coords, n * cap);
+    double* dle = st.out(lengths, n * cap);
+    int* dcn = st.out(counts, n);
+    int* dcr = st.out(crosses, n);
+    launch_lor_paths(g, sino_of(p, 1, 0), t, n, db, cap, dco, dle, dcn, dcr, cfg_of(c));
+    after_launch(c);
+    finish(c, st);
+  });
+}
+
+}  // extern "C"

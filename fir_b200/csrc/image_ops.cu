@@ -1,0 +1,247 @@
+// Image-space and sinogram-space element-wise kernels of the OSEM loop:
+// the gated EM update, the separable Gaussian filter with edge
+// renormalisation, the cylindrical cut, the mask, HU to mu conversion, and the
+// sinogram exponential / product.  All float arithmetic uses explicit
+// round-to-nearest intrinsics (no FMA contraction) in FIR's operation order,
+// so results are bit-identical to FIR's.
+#include "internal.h"
+
+namespace fir
+{
+namespace
+{
+constexpr int kBlock = 256;
+
+unsigned blocks_for(long long n, int block = kBlock)
+{
+  return (unsigned)((n + block - 1) / block);
+}
+
+// VolData::operator/= then VolData::operator*= (VolData.cc:305-343), as used
+// by reconAlgos.cc:161-166: bp <- bp/sens and img <- img*bp, each gated by
+// both operands exceeding 1e-5.  bp is left holding the quotient.
+__global__ void k_em_update(long long n, float* __restrict__ img, float* __restrict__ bp,
+                            const float* __restrict__ sens)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n)
+  {
+    return;
+  }
+  const float b = bp[i];
+  const float s = __ldg(sens + i);
+  const float q = ((double)b > kEps && (double)s > kEps) ? __fdiv_rn(b, s) : 0.0f;
+  const float x = img[i];
+  img[i] = ((double)x > kEps && (double)q > kEps) ? __fmul_rn(x, q) : 0.0f;
+  bp[i] = q;
+}
+
+// One pass of operations::convolve (operations.cc:84-156): sum and weight
+// norm over the in-bounds taps, accumulated in float in tap order, then
+// sum / norm.
+__global__ void k_conv_pass(int nx, int ny, int nz, int axis, Taps taps, const float* __restrict__ in,
+                            float* __restrict__ out)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = (long long)nx * ny * nz;
+  if (i >= n)
+  {
+    return;
+  }
+  const int x = (int)(i % nx);
+  const int y = (int)((i / nx) % ny);
+  const int z = (int)(i / ((long long)nx * ny));
+  const int coord = axis == 0 ? x : (axis == 1 ? y : z);
+  const int len = axis == 0 ? nx : (axis == 1 ? ny : nz);
+  const long long stride = axis == 0 ? 1 : (axis == 1 ? (long long)nx : (long long)nx * ny);
+  float sum = 0.0f, norm = 0.0f;
+  for (int k = -taps.half; k <= taps.half; ++k)
+  {
+    const int c = coord + k;
+    if (c >= 0 && c < len)
+    {
+      const float kv = taps.w[taps.half + k];
+      sum = __fadd_rn(sum, __fmul_rn(kv, __ldg(in + i + k * stride)));
+      norm = __fadd_rn(norm, kv);
+    }
+  }
+  if (norm > 0.0f)
+  {
+    out[i] = __fdiv_rn(sum, norm);
+  }
+}
+
+__device__ __forceinline__ double radius_of(int x, int y, int nx, int ny, double vx, double vy)
+{
+  // operations.cc:160-185 and :206-212: voxel centre relative to the volume
+  // centre, in double.
+  const double px = __dsub_rn(__dadd_rn(__dmul_rn((double)x, vx), __ddiv_rn(vx, 2.0)),
+                              __ddiv_rn(__dmul_rn((double)nx, vx), 2.0));
+  const double py = __dsub_rn(__dadd_rn(__dmul_rn((double)y, vy), __ddiv_rn(vy, 2.0)),
+                              __ddiv_rn(__dmul_rn((double)ny, vy), 2.0));
+  return __dsqrt_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)));
+}
+
+__global__ void k_conv_restore(int nx, int ny, int nz, double vx, double vy, float cut, float fwhm,
+                               const float* __restrict__ copy, float* __restrict__ img)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nx * ny * nz)
+  {
+    return;
+  }
+  const int x = (int)(i % nx);
+  const int y = (int)((i / nx) % ny);
+  // cutRadius - 5.0 * fwhm: float cut radius widened, double product.
+  if (radius_of(x, y, nx, ny, vx, vy) >= __dsub_rn((double)cut, __dmul_rn(5.0, (double)fwhm)))
+  {
+    img[i] = copy[i];
+  }
+}
+
+__global__ void k_cut_circle(int nx, int ny, int nz, double vx, double vy, float cut, float* img)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nx * ny * nz)
+  {
+    return;
+  }
+  const int x = (int)(i % nx);
+  const int y = (int)((i / nx) % ny);
+  if (radius_of(x, y, nx, ny, vx, vy) > (double)cut)
+  {
+    img[i] = 0.0f;
+  }
+}
+
+// operations::applyMask (operations.cc:222-241).
+__global__ void k_apply_mask(long long n, float* img, const float* __restrict__ mask)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n && __ldg(mask + i) <= 0.0f)
+  {
+    img[i] = 0.0f;
+  }
+}
+
+// operations::HounsfieldToMuMap (operations.cc:243-284): piecewise linear,
+// float arithmetic, water mu = 0.0096/mm.
+__global__ void k_hu_to_mu(long long n, float* img)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n)
+  {
+    return;
+  }
+  const float water = 0.0096f;
+  const float s1 = __fdiv_rn(water, 1000.0f);
+  const float s2 = __fdiv_rn(__fsub_rn(0.015f, water), 1000.0f);
+  float v = img[i];
+  if ((double)v <= -1000.0)
+  {
+    v = 0.0f;
+  }
+  else if ((double)v <= 0.0)
+  {
+    v = __fadd_rn(__fmul_rn(v, s1), water);
+  }
+  else
+  {
+    v = __fadd_rn(__fmul_rn(v, s2), water);
+  }
+  img[i] = v;
+}
+
+// ProjData::exponential (ProjData.cc:514-539).
+__global__ void k_exponential(long long n, float* sino)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n)
+  {
+    const float v = sino[i];
+    sino[i] = (double)v > kEps ? __double2float_rn(exp((double)v)) : 1.0f;
+  }
+}
+
+// ProjData::operator*= (ProjData.cc:481-512).
+__global__ void k_proj_multiply(long long n, float* a, const float* __restrict__ b)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n)
+  {
+    const float x = a[i], y = __ldg(b + i);
+    a[i] = ((double)x > kEps && (double)y > kEps) ? __fmul_rn(x, y) : 0.0f;
+  }
+}
+}  // namespace
+
+void launch_em_update(long long n, float* img, float* bp, const float* sens, const LaunchCfg& cfg)
+{
+  if (n > 0)
+  {
+    k_em_update<<<blocks_for(n), kBlock, 0, cfg.stream>>>(n, img, bp, sens);
+  }
+}
+
+void launch_conv_pass(int nx, int ny, int nz, int axis, const Taps& taps, const float* in, float* out,
+                      const LaunchCfg& cfg)
+{
+  const long long n = (long long)nx * ny * nz;
+  if (n > 0)
+  {
+    k_conv_pass<<<blocks_for(n), kBlock, 0, cfg.stream>>>(nx, ny, nz, axis, taps, in, out);
+  }
+}
+
+void launch_conv_restore(int nx, int ny, int nz, double vx, double vy, float cut, float fwhm,
+                         const float* copy, float* img, const LaunchCfg& cfg)
+{
+  const long long n = (long long)nx * ny * nz;
+  if (n > 0)
+  {
+    k_conv_restore<<<blocks_for(n), kBlock, 0, cfg.stream>>>(nx, ny, nz, vx, vy, cut, fwhm, copy, img);
+  }
+}
+
+void launch_cut_circle(int nx, int ny, int nz, double vx, double vy, float cut, float* img,
+                       const LaunchCfg& cfg)
+{
+  const long long n = (long long)nx * ny * nz;
+  if (n > 0)
+  {
+    k_cut_circle<<<blocks_for(n), kBlock, 0, cfg.stream>>>(nx, ny, nz, vx, vy, cut, img);
+  }
+}
+
+void launch_apply_mask(long long n, float* img, const float* mask, const LaunchCfg& cfg)
+{
+  if (n > 0)
+  {
+    k_apply_mask<<<blocks_for(n), kBlock, 0, cfg.stream>>>(n, img, mask);
+  }
+}
+
+void launch_hu_to_mu(long long n, float* img, const LaunchCfg& cfg)
+{
+  if (n > 0)
+  {
+    k_hu_to_mu<<<blocks_for(n), kBlock, 0, cfg.stream>>>(n, img);
+  }
+}
+
+void launch_exponential(long long n, float* sino, const LaunchCfg& cfg)
+{
+  if (n > 0)
+  {
+    k_exponential<<<blocks_for(n), kBlock, 0, cfg.stream>>>(n, sino);
+  }
+}
+
+void launch_proj_multiply(long long n, float* a, const float* b, const LaunchCfg& cfg)
+{
+  if (n > 0)
+  {
+    k_proj_multiply<<<blocks_for(n), kBlock, 0, cfg.stream>>>(n, a, b);
+  }
+}
+}  // namespace fir

@@ -1,0 +1,296 @@
+// Ray-driven projector kernels: forward projection (gather), backprojection
+// and sensitivity (scatter), the fused OSEM sub-iteration, and path dumps.
+//
+// Work decomposition: one thread per line of response.  Consecutive threads
+// take consecutive bins of FIR's enumeration, i.e. neighbouring tangential
+// bins of one view and axial plane, so a warp holds a bundle of 32 nearly
+// parallel, adjacent LORs: their traversals have near-equal trip counts and
+// touch neighbouring voxels, which keeps the warp converged and the image
+// gathers and scatters within a few L1/L2 sectors.  Paths are recomputed on
+// the fly (no LOR cache, no stored path), and the image (tens of MB) stays
+// resident in the 126 MB L2.
+#include "internal.h"
+
+namespace fir
+{
+namespace
+{
+__device__ __forceinline__ void flag(int* check, int bit)
+{
+  if (check != nullptr)
+  {
+    atomicOr(check, bit);
+  }
+}
+
+// projections::forward (projections.cc:15-92) with
+// VolData::computeLineIntegral (VolData.cc:357-371); optional epilogue
+// ProjData::exponential (ProjData.cc:514-539).
+template<FwdEpilogue EP>
+__global__ void __launch_bounds__(256) k_forward(Grid g, Sino s, Tables t,
+                                                 const float* __restrict__ img,
+                                                 float* __restrict__ sino, int* check)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n_enum)
+  {
+    return;
+  }
+  const Lor l = decode_bin(s, i);
+  double e[6];
+  lor_ends(s, t, l, e);
+  float line = 0.0f;
+  Walk w;
+  if (siddon_setup(g, e, w))
+  {
+    const bool ok = siddon_walk(
+      g,
+      w,
+      [&](int c, double len) { line = accumulate(line, len, __ldg(img + c)); });
+    if (!ok)
+    {
+      flag(check, kCheckWalkGuard);
+    }
+  }
+  if (EP == FwdEpilogue::Exp)
+  {
+    // exp evaluated in double and rounded once: the correctly rounded float
+    // exponential that FIR's std::exp(float) returns (ProjData.cc:531).
+    line = (double)line > kEps ? __double2float_rn(exp((double)line)) : 1.0f;
+  }
+  sino[l.bin] = line;
+}
+
+// projections::backward (projections.cc:94-184) with
+// VolData::projectLineIntegral (VolData.cc:373-385).  sino == nullptr is the
+// all-ones sinogram of computeSensitivityVol (projections.cc:186-197).
+__global__ void __launch_bounds__(256) k_backward(Grid g, Sino s, Tables t,
+                                                  const float* __restrict__ sino, float* img,
+                                                  int skip_zero, int* check)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n_enum)
+  {
+    return;
+  }
+  const Lor l = decode_bin(s, i);
+  const float val = sino != nullptr ? __ldg(sino + l.bin) : 1.0f;
+  if (skip_zero && val == 0.0f)
+  {
+    return;
+  }
+  double e[6];
+  lor_ends(s, t, l, e);
+  Walk w;
+  if (siddon_setup(g, e, w))
+  {
+    const double v = (double)val;
+    const bool ok = siddon_walk(
+      g,
+      w,
+      [&](int c, double len) { atomicAdd(img + c, __double2float_rn(dmul(len, v))); });
+    if (!ok)
+    {
+      flag(check, kCheckWalkGuard);
+    }
+  }
+}
+
+// The per-LOR body of one OSEM sub-iteration (reconAlgos.cc:119-158 with
+// getLine :11-59): project the current image along the LOR, add the bias,
+// and if the estimate exceeds 1e-5 backproject measured/estimated along the
+// same path.  The path is traversed twice from the same saved setup, so both
+// traversals visit identical voxels with identical lengths.
+__global__ void __launch_bounds__(256) k_osem_subset(Grid g, Sino s, Tables t,
+                                                     const float* __restrict__ img,
+                                                     const float* __restrict__ sino,
+                                                     const float* __restrict__ bias, float* bp,
+                                                     int skip_zero, int* check)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n_enum)
+  {
+    return;
+  }
+  const Lor l = decode_bin(s, i);
+  const float y = __ldg(sino + l.bin);
+  // With y == 0 the ratio is exactly 0 whatever the estimate, so the bin
+  // contributes nothing: skipping it is exact.
+  if (skip_zero && y == 0.0f)
+  {
+    return;
+  }
+  double e[6];
+  lor_ends(s, t, l, e);
+  Walk w;
+  const bool crosses = siddon_setup(g, e, w);
+  float line = 0.0f;
+  if (crosses)
+  {
+    if (!siddon_walk(g, w, [&](int c, double len) { line = accumulate(line, len, __ldg(img + c)); }))
+    {
+      flag(check, kCheckWalkGuard);
+      return;
+    }
+  }
+  if (bias != nullptr)
+  {
+    line = __fadd_rn(line, __ldg(bias + l.bin));
+  }
+  if (crosses && (double)line > kEps)
+  {
+    const double ratio = (double)__fdiv_rn(y, line);
+    siddon_walk(g, w, [&](int c, double len) { atomicAdd(bp + c, __double2float_rn(dmul(len, ratio))); });
+  }
+}
+
+__global__ void k_siddon_paths(Grid g, long long n, const double* __restrict__ ends, int cap,
+                               int* coords, double* lengths, int* counts, int* crosses, int* check)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n)
+  {
+    return;
+  }
+  double e[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+  {
+    e[k] = ends[6 * i + k];
+  }
+  Walk w;
+  int k = 0;
+  const bool c = siddon_setup(g, e, w);
+  if (c)
+  {
+    int* co = coords + i * cap;
+    double* le = lengths + i * cap;
+    if (!siddon_walk(g, w, [&](int v, double len) {
+          if (k < cap)
+          {
+            co[k] = v;
+            le[k] = len;
+          }
+          ++k;
+        }))
+    {
+      flag(check, kCheckWalkGuard);
+    }
+  }
+  counts[i] = k;
+  crosses[i] = c ? 1 : 0;
+}
+
+__global__ void k_lor_paths(Grid g, Sino s, Tables t, long long n, const long long* __restrict__ bins,
+                            int cap, int* coords, double* lengths, int* counts, int* crosses,
+                            int* check)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n)
+  {
+    return;
+  }
+  // bins are flat file-order indices: enumerate with one subset.
+  const long long b = bins[i];
+  if (b < 0 || b >= s.n_enum)
+  {
+    counts[i] = 0;
+    crosses[i] = 0;
+    return;
+  }
+  const Lor l = decode_bin(s, (int)b);
+  double e[6];
+  lor_ends(s, t, l, e);
+  Walk w;
+  int k = 0;
+  const bool c = siddon_setup(g, e, w);
+  if (c)
+  {
+    int* co = coords + i * cap;
+    double* le = lengths + i * cap;
+    if (!siddon_walk(g, w, [&](int v, double len) {
+          if (k < cap)
+          {
+            co[k] = v;
+            le[k] = len;
+          }
+          ++k;
+        }))
+    {
+      flag(check, kCheckWalkGuard);
+    }
+  }
+  counts[i] = k;
+  crosses[i] = c ? 1 : 0;
+}
+
+unsigned blocks_for(long long n, int block)
+{
+  return (unsigned)((n + block - 1) / block);
+}
+}  // namespace
+
+void launch_forward(const Grid& g, const Sino& s, const Tables& t, const float* img, float* sino,
+                    FwdEpilogue ep, const LaunchCfg& cfg)
+{
+  if (s.n_enum == 0)
+  {
+    return;
+  }
+  const unsigned nb = blocks_for(s.n_enum, cfg.block);
+  if (ep == FwdEpilogue::Exp)
+  {
+    k_forward<FwdEpilogue::Exp><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, sino, cfg.check);
+  }
+  else
+  {
+    k_forward<FwdEpilogue::None><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, sino, cfg.check);
+  }
+}
+
+void launch_backward(const Grid& g, const Sino& s, const Tables& t, const float* sino, float* img,
+                     bool skip_zero, const LaunchCfg& cfg)
+{
+  if (s.n_enum == 0)
+  {
+    return;
+  }
+  k_backward<<<blocks_for(s.n_enum, cfg.block), cfg.block, 0, cfg.stream>>>(
+    g, s, t, sino, img, skip_zero ? 1 : 0, cfg.check);
+}
+
+void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const float* img,
+                        const float* sino, const float* bias, float* bp, bool skip_zero,
+                        const LaunchCfg& cfg)
+{
+  if (s.n_enum == 0)
+  {
+    return;
+  }
+  k_osem_subset<<<blocks_for(s.n_enum, cfg.block), cfg.block, 0, cfg.stream>>>(
+    g, s, t, img, sino, bias, bp, skip_zero ? 1 : 0, cfg.check);
+}
+
+void launch_siddon_paths(const Grid& g, long long n, const double* ends, int cap, int* coords,
+                         double* lengths, int* counts, int* crosses, const LaunchCfg& cfg)
+{
+  if (n == 0)
+  {
+    return;
+  }
+  k_siddon_paths<<<blocks_for(n, 128), 128, 0, cfg.stream>>>(g, n, ends, cap, coords, lengths, counts,
+                                                             crosses, cfg.check);
+}
+
+void launch_lor_paths(const Grid& g, const Sino& s, const Tables& t, long long n,
+                      const long long* bins, int cap, int* coords, double* lengths, int* counts,
+                      int* crosses, const LaunchCfg& cfg)
+{
+  if (n == 0)
+  {
+    return;
+  }
+  k_lor_paths<<<blocks_for(n, 128), 128, 0, cfg.stream>>>(g, s, t, n, bins, cap, coords, lengths, counts,
+                                                          crosses, cfg.check);
+}
+}  // namespace fir

@@ -1,0 +1,303 @@
+// Device-side geometry and the Siddon traversal of FIR (src_lib/Siddon.cc).
+//
+// The traversal reproduces FIR's double-precision arithmetic operation by
+// operation: every add, multiply, divide and square root is an explicit
+// round-to-nearest intrinsic (never fused into an FMA), extents, planes and
+// tie tolerance are FIR's, and the loop visits and emits exactly the voxels
+// FIR's computePath emits, with the same lengths.  The voxel index lists are
+// therefore bit-identical to FIR's.
+#pragma once
+
+#include <cstdint>
+
+namespace fir
+{
+constexpr double kEps = 0.00001;   // macros.h:8
+constexpr int kMaxSegments = 255;  // 2*128-1 segments: up to 128 rings at span 1
+
+// Volume grid as the traversal sees it (Siddon.cc:20-63).
+struct Grid
+{
+  int nx, ny, nz, nxy;
+  double ext[3];   // step sizes: FIR's int-truncated extents, or the real ones
+  double low[3];   // border planes: x,y = offset - voxel/2, z = offset - depth/2
+  double high[3];  // low + n * voxel (real voxel extents, as in FIR)
+};
+
+// Sinogram enumeration for one launch.  Bins are enumerated segment by
+// segment in FIR's order; inside a segment, subset-local index r maps to
+// view = (r / binsPerView) * nSubsets + subset (LORCache.cc:115-133).
+struct Sino
+{
+  int n_rings, n_cpr, span, half_span;
+  int n_segments, seg_offset, tang_offset, n_views, n_tang;
+  int n_subsets, subset;
+  int n_enum;                          // bins enumerated by this launch
+  int seg_base[kMaxSegments + 1];      // first flat bin of each segment (file order)
+  int enum_base[kMaxSegments + 1];     // first enumerated index of each segment
+  int n_axial[kMaxSegments];
+};
+
+struct Tables
+{
+  const double2* xy;  // crystal centres of one ring (ScannerData.cc:248-329)
+  const double* z;    // slice centres, 2*nRings-1 (ScannerData.cc:331-377)
+};
+
+struct Lor
+{
+  int bin;     // flat bin index (file order)
+  int seg, view, axial, tang;
+};
+
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+
+// Enumerated index -> bin coordinates.
+__device__ __forceinline__ Lor decode_bin(const Sino& s, int i)
+{
+  int lo = 0, hi = s.n_segments;
+  while (hi - lo > 1)
+  {
+    const int mid = (lo + hi) >> 1;
+    if (s.enum_base[mid] <= i)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const int r = i - s.enum_base[lo];
+  const int nax = s.n_axial[lo];
+  const int bpv = nax * s.n_tang;
+  const int sv = r / bpv;
+  const int rem = r - sv * bpv;
+  const int ax = rem / s.n_tang;
+  Lor l;
+  l.view = sv * s.n_subsets + s.subset;
+  l.seg = lo - s.seg_offset;
+  l.axial = ax;
+  l.tang = rem - ax * s.n_tang - s.tang_offset;
+  l.bin = s.seg_base[lo] + l.view * bpv + rem;
+  return l;
+}
+
+// ProjData::getCrystalAxialCoord (ProjData.cc:198-299): slice indices.
+__device__ __forceinline__ void crystal_axial(const Sino& s, int seg, int axial, int& a1, int& a2)
+{
+  if (s.span == 1)
+  {
+    if (seg == 0)
+    {
+      a1 = a2 = 2 * axial;
+    }
+    else if (seg > 0)
+    {
+      a1 = 2 * (axial + seg);
+      a2 = 2 * axial;
+    }
+    else
+    {
+      a1 = 2 * axial;
+      a2 = 2 * (axial - seg);
+    }
+    return;
+  }
+  if (seg == 0)
+  {
+    a1 = a2 = axial;
+    return;
+  }
+  const int aseg = seg < 0 ? -seg : seg;
+  const int mid = aseg * s.span;
+  const int h = s.half_span;
+  if (axial < h)
+  {
+    const int rd = mid - h + axial;
+    a1 = seg > 0 ? 2 * rd : 0;
+    a2 = seg > 0 ? 0 : 2 * rd;
+    return;
+  }
+  const int inv = s.n_axial[seg + s.seg_offset] - axial - 1;
+  if (inv < h)
+  {
+    const int rd = mid - h + inv;
+    const int smax = 2 * s.n_rings - 2;
+    a1 = seg > 0 ? smax : smax - 2 * rd;
+    a2 = seg > 0 ? smax - 2 * rd : smax;
+    return;
+  }
+  const int adj = axial - h;
+  a1 = seg > 0 ? 2 * mid + adj : adj;
+  a2 = seg > 0 ? adj : 2 * mid + adj;
+}
+
+// ProjData::getCrystalAngCoord (ProjData.cc:301-340).
+__device__ __forceinline__ void crystal_ang(const Sino& s, int view, int tang, int& c1, int& c2)
+{
+  const int shift = tang >= 0 ? tang / 2 : (tang - 1) / 2;
+  const int odd = (tang < 0 ? -tang : tang) & 1;
+  int a = view + shift + odd;
+  int b = view + s.n_views - shift;
+  if (a < 0)
+    a += s.n_cpr;
+  else if (a >= s.n_cpr)
+    a -= s.n_cpr;
+  if (b < 0)
+    b += s.n_cpr;
+  else if (b >= s.n_cpr)
+    b -= s.n_cpr;
+  c1 = a;
+  c2 = b;
+}
+
+__device__ __forceinline__ void lor_ends(const Sino& s, const Tables& t, const Lor& l, double e[6])
+{
+  int a1, a2, c1, c2;
+  crystal_axial(s, l.seg, l.axial, a1, a2);
+  crystal_ang(s, l.view, l.tang, c1, c2);
+  const double2 p1 = __ldg(t.xy + c1);
+  const double2 p2 = __ldg(t.xy + c2);
+  e[0] = p1.x;
+  e[1] = p1.y;
+  e[2] = __ldg(t.z + a1);
+  e[3] = p2.x;
+  e[4] = p2.y;
+  e[5] = __ldg(t.z + a2);
+}
+
+// State of one path between two plane crossings.
+struct Walk
+{
+  double a[3];   // alpha of the next plane crossing in each dimension
+  double da[3];  // alpha between neighbouring planes
+  int pos[3];    // current voxel
+  int dir[3];
+  double amin, amax, d12;
+};
+
+// Siddon::computePath setup (Siddon.cc:112-203 with dimSetup :260-317,
+// getEntryExit :319-334, getStartInd :336-350, prepareDim :352-377).
+// Returns false when the segment misses the volume.
+__device__ __forceinline__ bool siddon_setup(const Grid& g, const double e[6], Walk& w)
+{
+  double diff[3], smin[3], smax[3], snext[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    const double c1 = e[d], c2 = e[3 + d];
+    const double lo = g.low[d], hi = g.high[d];
+    double df = dsub(c2, c1);
+    if (fabs(df) > kEps)
+    {
+      if (df > 0)
+      {
+        w.dir[d] = 1;
+        smin[d] = ddiv(dsub(lo, c1), df);
+        smax[d] = ddiv(dsub(hi, c1), df);
+      }
+      else
+      {
+        w.dir[d] = -1;
+        smin[d] = ddiv(dsub(hi, c1), df);
+        smax[d] = ddiv(dsub(lo, c1), df);
+      }
+      snext[d] = 0.0;
+    }
+    else
+    {
+      if (c1 < lo || c1 > hi)
+      {
+        return false;
+      }
+      df = kEps;
+      w.dir[d] = -1;
+      smin[d] = 0.0;
+      smax[d] = 1.0;
+      snext[d] = 1.0;
+    }
+    diff[d] = df;
+  }
+  // MAX(a, MAX(b, MAX(c, 0))) and MIN(a, MIN(b, MIN(c, 1))), macros.h:4-5
+  double t = smin[2] > 0.0 ? smin[2] : 0.0;
+  t = smin[1] > t ? smin[1] : t;
+  w.amin = smin[0] > t ? smin[0] : t;
+  t = smax[2] < 1.0 ? smax[2] : 1.0;
+  t = smax[1] < t ? smax[1] : t;
+  w.amax = smax[0] < t ? smax[0] : t;
+  if (w.amin >= w.amax)
+  {
+    return false;
+  }
+  const int nm1[3] = {g.nx - 1, g.ny - 1, g.nz - 1};
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    w.da[d] = ddiv(g.ext[d], fabs(diff[d]));
+  }
+  w.d12 = __dsqrt_rn(dadd(dadd(dmul(diff[0], diff[0]), dmul(diff[1], diff[1])), dmul(diff[2], diff[2])));
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    int ind = __double2int_rz(ddiv(dsub(dadd(e[d], dmul(diff[d], w.amin)), g.low[d]), g.ext[d]));
+    ind = ind < nm1[d] ? ind : nm1[d];
+    w.pos[d] = ind > 0 ? ind : 0;
+    double al = snext[d];
+    if (al < 1.0)
+    {
+      al = ddiv(dsub(dadd(g.low[d], dmul(g.ext[d], (double)w.pos[d])), e[d]), diff[d]);
+    }
+    if (w.dir[d] > 0)
+    {
+      al = dadd(al, w.da[d]);
+    }
+    w.a[d] = al;
+  }
+  return true;
+}
+
+// The computePath loop (Siddon.cc:207-252).  emit(linearIndex, length) is
+// called for every element FIR would store, in FIR's order.  Returns false
+// if the iteration bound (a path can cross at most nx+ny+nz+3 planes) was
+// hit, which only non-finite input can cause.
+template<class Emit>
+__device__ __forceinline__ bool siddon_walk(const Grid& g, Walk w, Emit&& emit)
+{
+  double prev = w.amin;
+  int guard = g.nx + g.ny + g.nz + 4;
+  while (prev < w.amax)
+  {
+    if (--guard < 0)
+    {
+      return false;
+    }
+    // MIN(alphaMax, MIN(ax, MIN(ay, az))); fmin differs from the macro only
+    // in the sign of a zero result, which no emitted value depends on.
+    const double next = fmin(w.amax, fmin(w.a[0], fmin(w.a[1], w.a[2])));
+    if ((unsigned)w.pos[0] < (unsigned)g.nx && (unsigned)w.pos[1] < (unsigned)g.ny &&
+        (unsigned)w.pos[2] < (unsigned)g.nz)
+    {
+      emit(w.pos[0] + w.pos[1] * g.nx + w.pos[2] * g.nxy, dmul(dsub(next, prev), w.d12));
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+      if (fabs(dsub(w.a[d], next)) < kEps)
+      {
+        w.a[d] = dadd(w.a[d], w.da[d]);
+        w.pos[d] += w.dir[d];
+      }
+    }
+    prev = next;
+  }
+  return true;
+}
+
+// VolData::computeLineIntegral accumulation step (VolData.cc:362-368): the
+// float running sum is widened, the double product added, the sum rounded.
+__device__ __forceinline__ float accumulate(float line, double length, float value)
+{
+  return __double2float_rn(dadd((double)line, dmul(length, (double)value)));
+}
+
+}  // namespace fir

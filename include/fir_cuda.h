@@ -1,0 +1,258 @@
+/*
+ * fir_cuda.h -- C ABI of the B200 (sm_100a) implementation of FIR's
+ * projection and reconstruction path.
+ *
+ * This is the drop-in boundary.  It replaces, call for call, the C++ entry
+ * points of FIR's L4 layer (paths inside the FIR project):
+ *
+ *   fir_forward            projections::forward            src_lib/projections.h:9-12, projections.cc:15-92
+ *   fir_backward           projections::backward           src_lib/projections.h:14-18, projections.cc:94-184
+ *   fir_sensitivity        projections::computeSensitivityVol  src_lib/projections.h:20-24, projections.cc:186-197
+ *   fir_osem_subiteration  one sub-iteration of reconAlgos::OSEM  src_lib/reconAlgos.cc:119-198
+ *   fir_osem               reconAlgos::OSEM                src_lib/reconAlgos.h:29-36, reconAlgos.cc:63-201
+ *   fir_convolve           operations::convolve            src_lib/operations.h:7-10, operations.cc:11-192
+ *   fir_cut_circle         operations::cutCircle           src_lib/operations.h:13-15, operations.cc:194-220
+ *   fir_apply_mask         operations::applyMask           src_lib/operations.h:19, operations.cc:222-241
+ *   fir_hu_to_mu           operations::HounsfieldToMuMap   src_lib/operations.h:22, operations.cc:243-284
+ *   fir_proj_exponential   ProjData::exponential           src_lib/ProjData.h:108, ProjData.cc:514-539
+ *   fir_proj_multiply      ProjData::operator*=            src_lib/ProjData.h:107, ProjData.cc:481-512
+ *   fir_em_update          VolData /=, *= of the EM update src_lib/VolData.cc:305-343, reconAlgos.cc:161-166
+ *   fir_lor_paths          Siddon::computePathBetweenCrystals (path dump) src_lib/Siddon.cc:88-258
+ *   fir_siddon_paths       Siddon::computePath (path dump) src_lib/Siddon.h:45-55
+ *   fir_proj_geometry      ProjHeader::check + ProjGeometry::fill  src_lib/ProjHeader.cc:6-186
+ *   fir_scanner_tables     ScannerHeader::check + ScannerData position tables  src_lib/ScannerHeader.cc:26-342, ScannerData.cc:248-377
+ *
+ * Conventions
+ *   - Every entry point returns a fir_status; FIR_OK is 0.  On failure
+ *     fir_last_error() returns the message (thread-local), worded as FIR's
+ *     own error() text where FIR has one.  No entry point throws.
+ *   - Data pointers may be device pointers (work is enqueued on the context's
+ *     stream and the call returns without waiting) or host pointers (the
+ *     library stages them through device memory it owns, and the call
+ *     returns when the results are back in host memory).
+ *   - Sinograms are float32, segments -segOffset..+segOffset concatenated,
+ *     each [view][axial][tang] (FIR's file order, ProjInterfileReader.cc:78-93).
+ *     Volumes are float32 [frame][z][y][x] (VolData.h:151-156).
+ *   - One context per host thread or stream; calls on different contexts
+ *     may run concurrently.  A context is not thread-safe.
+ */
+#ifndef FIR_CUDA_H
+#define FIR_CUDA_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FIR_CUDA_ABI_VERSION 1
+
+typedef enum fir_status
+{
+  FIR_OK = 0,
+  FIR_ERR_INVALID_ARGUMENT = 1, /* header or parameter rejected (FIR's error()) */
+  FIR_ERR_CUDA = 2,             /* a CUDA runtime call failed */
+  FIR_ERR_OUT_OF_MEMORY = 3,
+  FIR_ERR_DEVICE_CHECK = 4,     /* a device-side check tripped (see message) */
+  FIR_ERR_NO_DEVICE = 5,
+  FIR_ERR_NOT_SUPPORTED = 6
+} fir_status;
+
+/* VolHeader (src_lib/VolHeader.h:7-23).  offset_x/y: centre of the first
+ * voxel; offset_z: z offset of the volume centre from the scanner centre. */
+typedef struct fir_vol_desc
+{
+  int nx, ny, nz;
+  double voxel_x, voxel_y, voxel_z;
+  double offset_x, offset_y, offset_z;
+  int n_frames;
+} fir_vol_desc;
+
+/* ProjHeader (src_lib/ProjHeader.h:15-40).  n_tang_coords = 0 selects the
+ * maximum, n_crystals_per_ring - 1. */
+typedef struct fir_proj_desc
+{
+  int n_rings;
+  int n_crystals_per_ring;
+  int segment_span;
+  int n_segments;
+  int n_tang_coords;
+} fir_proj_desc;
+
+/* ProjGeometry (src_lib/ProjHeader.h:42-80); n_axial is returned separately. */
+typedef struct fir_proj_info
+{
+  long long n_bins;
+  int seg_offset;
+  int tang_offset;
+  int n_views;
+  int half_span;
+  int max_ring_diff;
+  int n_tang_coords;
+} fir_proj_info;
+
+/* ScannerHeader (src_lib/ScannerHeader.h:7-46); zero dimensions mean "fit
+ * tightly on the level below". */
+typedef struct fir_scanner_desc
+{
+  double crystal_dims[3];
+  int crystal_repeat[2];
+  double inter_crystal[2];
+  double module_dims[3];
+  int module_repeat[2];
+  double inter_module[2];
+  double rsector_dims[3];
+  int rsector_repeat;
+  double rsector_inner_radius;
+} fir_scanner_desc;
+
+/* OSEMCoreParams (src_lib/reconAlgos.h:9-22). */
+typedef struct fir_osem_params
+{
+  int n_iterations;
+  int n_subsets;
+  int save_interval;
+  float cut_radius;
+  int convolution_interval;
+  float fwhm_xyz[3];
+} fir_osem_params;
+
+typedef struct fir_ctx fir_ctx;
+
+/* Context options (fir_ctx_set_option). */
+typedef enum fir_option
+{
+  /* FIR_GEOMETRY_REFERENCE (default): voxel extents are truncated to whole
+   * millimetres for the traversal, exactly as FIR stores them in int
+   * (Siddon.h:15-16,113).  FIR_GEOMETRY_EXACT: real-valued extents.  The two
+   * agree for integer voxel sizes. */
+  FIR_OPT_GEOMETRY = 1,
+  /* FIR_BACKPROJ_ATOMIC (default): float atomics, order-nondeterministic
+   * like FIR's "omp atomic".  FIR_BACKPROJ_DETERMINISTIC: contributions are
+   * sorted per voxel into FIR's serial LOR order and summed in that order
+   * with FIR's rounding, reproducing a single-threaded FIR run. */
+  FIR_OPT_BACKPROJ_MODE = 2,
+  /* 1: skip sinogram bins whose value is exactly 0 in backprojection and
+   * OSEM (their contribution is exactly 0).  Default 0. */
+  FIR_OPT_SKIP_ZERO_BINS = 3,
+  /* Threads per block of the projector kernels (32..256, multiple of 32);
+   * 0 restores the default. */
+  FIR_OPT_BLOCK_SIZE = 4,
+  /* 1: bracket every projector-kernel launch (forward, backward,
+   * sensitivity, OSEM sub-iteration) with CUDA events on the context's
+   * stream; read the accumulated device time with fir_ctx_projector_time. */
+  FIR_OPT_TIMING = 5
+} fir_option;
+
+enum
+{
+  FIR_GEOMETRY_REFERENCE = 0,
+  FIR_GEOMETRY_EXACT = 1,
+  FIR_BACKPROJ_ATOMIC = 0,
+  FIR_BACKPROJ_DETERMINISTIC = 1
+};
+
+/* ---- library / host helpers (no GPU needed) ---- */
+int fir_abi_version(void);
+const char* fir_last_error(void);
+const char* fir_status_string(fir_status s);
+
+/* ProjHeader::check + ProjGeometry::fill.  desc->n_tang_coords = 0 is
+ * resolved in *geom.  n_axial: optional, room for desc->n_segments ints. */
+fir_status fir_proj_geometry(const fir_proj_desc* desc, fir_proj_info* geom, int* n_axial);
+
+/* ScannerHeader::check + ScannerData tables.  xy: 2*n_crystals_per_ring
+ * doubles (x,y interleaved); z: 2*n_rings-1 doubles (slice centres).  Either
+ * may be NULL to query n_rings / n_crystals_per_ring only. */
+fir_status fir_scanner_tables(const fir_scanner_desc* desc, double* xy, double* z, int* n_rings,
+                              int* n_crystals_per_ring);
+
+/* ---- contexts ---- */
+fir_status fir_ctx_create(fir_ctx** ctx, int device);
+fir_status fir_ctx_destroy(fir_ctx* ctx);
+/* stream: a cudaStream_t (NULL = legacy default stream). */
+fir_status fir_ctx_set_stream(fir_ctx* ctx, void* stream);
+fir_status fir_ctx_set_option(fir_ctx* ctx, fir_option opt, int value);
+fir_status fir_ctx_get_option(fir_ctx* ctx, fir_option opt, int* value);
+/* Uploads the scanner's crystal and slice position tables. */
+fir_status fir_ctx_set_scanner(fir_ctx* ctx, const fir_scanner_desc* scanner);
+/* Waits for the context's stream and reports device-side check failures. */
+fir_status fir_ctx_synchronize(fir_ctx* ctx);
+/* Number of kernels this context launched since creation (all entry points). */
+long long fir_ctx_launch_count(const fir_ctx* ctx);
+/* With FIR_OPT_TIMING on: waits for the recorded events and returns the total
+ * device time (ms) and number of projector-kernel launches since the last
+ * reset; reset != 0 clears the totals. */
+fir_status fir_ctx_projector_time(fir_ctx* ctx, double* ms, long long* launches, int reset);
+
+/* ---- projectors ---- */
+/* projections::forward: sino[b] = sum over the Siddon path of bin b of
+ * length * img, img being frame 0 of vol (VolData active frame 0). */
+fir_status fir_forward(fir_ctx* ctx, const fir_vol_desc* vol, const float* img,
+                       const fir_proj_desc* proj, float* sino);
+
+/* Forward projection of an attenuation map followed by FIR's
+ * ProjData::exponential in the same kernel: acf[b] = exp(line) if line >
+ * 1e-5, else 1 (the attenuation correction factors of src_bin/OSEM.cc:294-311,
+ * without the HU conversion). */
+fir_status fir_forward_exp(fir_ctx* ctx, const fir_vol_desc* vol, const float* mu,
+                           const fir_proj_desc* proj, float* acf);
+
+/* projections::backward: img (n_subsets frames) is zeroed, then the bins of
+ * subset s (views v with v % n_subsets == s) are backprojected into frame s. */
+fir_status fir_backward(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino,
+                        const fir_vol_desc* vol, float* img, int n_subsets);
+
+/* projections::computeSensitivityVol: backward of an all-ones sinogram. */
+fir_status fir_sensitivity(fir_ctx* ctx, const fir_proj_desc* proj, const fir_vol_desc* vol,
+                           float* sens, int n_subsets);
+
+/* ---- OSEM ---- */
+/* One sub-iteration of reconAlgos::OSEM (reconAlgos.cc:119-187): for every
+ * bin of subset `subset`, line = projection of img (+ bias), and if line >
+ * 1e-5 the ratio sino/line is backprojected; then img *= bp / sens_frame
+ * with FIR's 1e-5 gates, then the Gaussian filter if subiter %
+ * convolution_interval == 0, then the cylindrical cut.  subiter is the
+ * 1-based sub-iteration number.  bias may be NULL. */
+fir_status fir_osem_subiteration(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino,
+                                 const float* bias, const fir_vol_desc* vol, float* img,
+                                 const float* sens_frame, const fir_osem_params* params,
+                                 int subset, int subiter);
+
+/* Called by fir_osem after sub-iteration `subiter` when params->save_interval
+ * asks for an intermediate image; img is a host copy (nx*ny*nz floats). */
+typedef void (*fir_osem_save_fn)(void* user, int subiter, const float* img);
+
+/* reconAlgos::OSEM: the initial cut, then n_iterations x n_subsets
+ * sub-iterations.  sens holds n_subsets frames.  save may be NULL. */
+fir_status fir_osem(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const float* bias,
+                    const fir_vol_desc* vol, float* img, const float* sens,
+                    const fir_osem_params* params, fir_osem_save_fn save, void* user);
+
+/* ---- image and sinogram operations ---- */
+fir_status fir_em_update(fir_ctx* ctx, const fir_vol_desc* vol, float* img, float* bp,
+                         const float* sens_frame);
+/* operations::convolve on every frame of vol. */
+fir_status fir_convolve(fir_ctx* ctx, const fir_vol_desc* vol, float* img, const float fwhm_xyz[3],
+                        float cut_radius);
+fir_status fir_cut_circle(fir_ctx* ctx, const fir_vol_desc* vol, float* img, float cut_radius);
+fir_status fir_apply_mask(fir_ctx* ctx, const fir_vol_desc* vol, float* img, const float* mask);
+fir_status fir_hu_to_mu(fir_ctx* ctx, const fir_vol_desc* vol, float* img);
+fir_status fir_proj_exponential(fir_ctx* ctx, const fir_proj_desc* proj, float* sino);
+fir_status fir_proj_multiply(fir_ctx* ctx, const fir_proj_desc* proj, float* a, const float* b);
+
+/* ---- path dumps (debugging and parity checks) ---- */
+/* Siddon::computePath for n segments, ends[6*i..6*i+5] = (x1,y1,z1,x2,y2,z2).
+ * Row i of coords/lengths holds up to cap elements; counts[i] = elements of
+ * the path (may exceed cap), crosses[i] = 1 if the segment meets the volume. */
+fir_status fir_siddon_paths(fir_ctx* ctx, const fir_vol_desc* vol, long long n, const double* ends,
+                            int cap, int* coords, double* lengths, int* counts, int* crosses);
+/* Same for sinogram bins given by their flat index (file order). */
+fir_status fir_lor_paths(fir_ctx* ctx, const fir_proj_desc* proj, const fir_vol_desc* vol,
+                         long long n, const long long* bins, int cap, int* coords, double* lengths,
+                         int* counts, int* crosses);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FIR_CUDA_H */
