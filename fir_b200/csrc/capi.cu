@@ -605,6 +605,20 @@ Grid grid_of(const fir_ctx& c, const VolInfo& v)
   g.high[0] = g.low[0] + v.d.nx * v.d.voxel_x;
   g.high[1] = g.low[1] + v.d.ny * v.d.voxel_y;
   g.high[2] = g.low[2] + depth;
+  // Each traversal step consumes at least one plane crossing; a dimension
+  // has at most span/step + 2 crossings in [alphaMin, alphaMax] (a cancelled
+  // dimension two).  With FIR's truncated extents the step can be shorter
+  // than the voxel, so the bound is counted in steps, not voxels.
+  double bound = 8.0;
+  for (int d = 0; d < 3; ++d)
+  {
+    bound += std::ceil((g.high[d] - g.low[d]) / g.ext[d]) + 2.0;
+  }
+  if (!(bound < 1.0e9))
+  {
+    fail(FIR_ERR_NOT_SUPPORTED, "volume spans ", bound, " traversal steps");
+  }
+  g.guard = (int)bound;
   return g;
 }
 

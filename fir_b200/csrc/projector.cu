@@ -5,10 +5,12 @@
 // take consecutive bins of FIR's enumeration, i.e. neighbouring tangential
 // bins of one view and axial plane, so a warp holds a bundle of 32 nearly
 // parallel, adjacent LORs: their traversals have near-equal trip counts and
-// touch neighbouring voxels, which keeps the warp converged and the image
-// gathers and scatters within a few L1/L2 sectors.  Paths are recomputed on
-// the fly (no LOR cache, no stored path), and the image (tens of MB) stays
-// resident in the 126 MB L2.
+// touch neighbouring voxels, which keeps the gathers and scatters of a warp
+// step within a few L1/L2 sectors.  The traversal is warp-synchronous (see
+// siddon.cuh), so no lane leaves its warp; kernels therefore never return
+// early: lanes without work pass go = false to the traversal.  Paths are
+// recomputed on the fly (no LOR cache, no stored path) and the image (tens of
+// MB) stays resident in the 126 MB L2.
 #include "internal.h"
 
 namespace fir
@@ -32,33 +34,38 @@ __global__ void __launch_bounds__(256) k_forward(Grid g, Sino s, Tables t,
                                                  float* __restrict__ sino, int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= s.n_enum)
+  const bool valid = i < s.n_enum;
+  Lor l{};
+  Walk w{};
+  bool go = false;
+  if (valid)
   {
-    return;
+    l = decode_bin(s, i);
+    double e[6];
+    lor_ends(s, t, l, e);
+    go = siddon_setup(g, e, w);
   }
-  const Lor l = decode_bin(s, i);
-  double e[6];
-  lor_ends(s, t, l, e);
   float line = 0.0f;
-  Walk w;
-  if (siddon_setup(g, e, w))
-  {
-    const bool ok = siddon_walk(
-      g,
-      w,
-      [&](int c, double len) { line = accumulate(line, len, __ldg(img + c)); });
-    if (!ok)
+  const bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
+    if (inside)
     {
-      flag(check, kCheckWalkGuard);
+      line = accumulate(line, len, __ldg(img + c));
     }
-  }
-  if (EP == FwdEpilogue::Exp)
+  });
+  if (!ok)
   {
-    // exp evaluated in double and rounded once: the correctly rounded float
-    // exponential that FIR's std::exp(float) returns (ProjData.cc:531).
-    line = (double)line > kEps ? __double2float_rn(exp((double)line)) : 1.0f;
+    flag(check, kCheckWalkGuard);
   }
-  sino[l.bin] = line;
+  if (valid)
+  {
+    if (EP == FwdEpilogue::Exp)
+    {
+      // exp evaluated in double and rounded once: the correctly rounded float
+      // exponential that FIR's std::exp(float) returns (ProjData.cc:531).
+      line = (double)line > kEps ? __double2float_rn(exp((double)line)) : 1.0f;
+    }
+    sino[l.bin] = line;
+  }
 }
 
 // projections::backward (projections.cc:94-184) with
@@ -69,30 +76,31 @@ __global__ void __launch_bounds__(256) k_backward(Grid g, Sino s, Tables t,
                                                   int skip_zero, int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= s.n_enum)
+  Walk w{};
+  bool go = false;
+  double v = 0.0;
+  if (i < s.n_enum)
   {
-    return;
-  }
-  const Lor l = decode_bin(s, i);
-  const float val = sino != nullptr ? __ldg(sino + l.bin) : 1.0f;
-  if (skip_zero && val == 0.0f)
-  {
-    return;
-  }
-  double e[6];
-  lor_ends(s, t, l, e);
-  Walk w;
-  if (siddon_setup(g, e, w))
-  {
-    const double v = (double)val;
-    const bool ok = siddon_walk(
-      g,
-      w,
-      [&](int c, double len) { atomicAdd(img + c, __double2float_rn(dmul(len, v))); });
-    if (!ok)
+    const Lor l = decode_bin(s, i);
+    const float val = sino != nullptr ? __ldg(sino + l.bin) : 1.0f;
+    v = (double)val;
+    // with val == 0 every contribution is exactly 0
+    if (!(skip_zero && val == 0.0f))
     {
-      flag(check, kCheckWalkGuard);
+      double e[6];
+      lor_ends(s, t, l, e);
+      go = siddon_setup(g, e, w);
     }
+  }
+  const bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
+    if (inside)
+    {
+      atomicAdd(img + c, __double2float_rn(dmul(len, v)));
+    }
+  });
+  if (!ok)
+  {
+    flag(check, kCheckWalkGuard);
   }
 }
 
@@ -108,39 +116,76 @@ __global__ void __launch_bounds__(256) k_osem_subset(Grid g, Sino s, Tables t,
                                                      int skip_zero, int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= s.n_enum)
+  const bool valid = i < s.n_enum;
+  Lor l{};
+  Walk w{};
+  bool go = false;
+  float y = 0.0f;
+  if (valid)
   {
-    return;
-  }
-  const Lor l = decode_bin(s, i);
-  const float y = __ldg(sino + l.bin);
-  // With y == 0 the ratio is exactly 0 whatever the estimate, so the bin
-  // contributes nothing: skipping it is exact.
-  if (skip_zero && y == 0.0f)
-  {
-    return;
-  }
-  double e[6];
-  lor_ends(s, t, l, e);
-  Walk w;
-  const bool crosses = siddon_setup(g, e, w);
-  float line = 0.0f;
-  if (crosses)
-  {
-    if (!siddon_walk(g, w, [&](int c, double len) { line = accumulate(line, len, __ldg(img + c)); }))
+    l = decode_bin(s, i);
+    y = __ldg(sino + l.bin);
+    // With y == 0 the ratio is exactly 0 whatever the estimate, so the bin
+    // contributes nothing: skipping it is exact.
+    if (!(skip_zero && y == 0.0f))
     {
-      flag(check, kCheckWalkGuard);
-      return;
+      double e[6];
+      lor_ends(s, t, l, e);
+      go = siddon_setup(g, e, w);
     }
   }
-  if (bias != nullptr)
+  float line = 0.0f;
+  bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
+    if (inside)
+    {
+      line = accumulate(line, len, __ldg(img + c));
+    }
+  });
+  if (valid && bias != nullptr)
   {
     line = __fadd_rn(line, __ldg(bias + l.bin));
   }
-  if (crosses && (double)line > kEps)
+  const bool back = go && ok && (double)line > kEps;
+  const double ratio = back ? (double)__fdiv_rn(y, line) : 0.0;
+  ok = siddon_walk(g, w, back, [&](bool inside, int c, double len) {
+         if (inside)
+         {
+           atomicAdd(bp + c, __double2float_rn(dmul(len, ratio)));
+         }
+       }) && ok;
+  if (!ok)
   {
-    const double ratio = (double)__fdiv_rn(y, line);
-    siddon_walk(g, w, [&](int c, double len) { atomicAdd(bp + c, __double2float_rn(dmul(len, ratio))); });
+    flag(check, kCheckWalkGuard);
+  }
+}
+
+// Path dump of one segment into row i of coords / lengths.
+__device__ __forceinline__ void dump_path(const Grid& g, const Walk& w, bool go, long long i, int cap,
+                                          int* coords, double* lengths, int* counts, int* crosses,
+                                          bool valid, int* check)
+{
+  int k = 0;
+  int* co = coords + i * cap;
+  double* le = lengths + i * cap;
+  const bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
+    if (inside)
+    {
+      if (k < cap)
+      {
+        co[k] = c;
+        le[k] = len;
+      }
+      ++k;
+    }
+  });
+  if (!ok)
+  {
+    flag(check, kCheckWalkGuard);
+  }
+  if (valid)
+  {
+    counts[i] = k;
+    crosses[i] = go ? 1 : 0;
   }
 }
 
@@ -148,37 +193,20 @@ __global__ void k_siddon_paths(Grid g, long long n, const double* __restrict__ e
                                int* coords, double* lengths, int* counts, int* crosses, int* check)
 {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= n)
+  const bool valid = i < n;
+  Walk w{};
+  bool go = false;
+  if (valid)
   {
-    return;
-  }
-  double e[6];
+    double e[6];
 #pragma unroll
-  for (int k = 0; k < 6; ++k)
-  {
-    e[k] = ends[6 * i + k];
-  }
-  Walk w;
-  int k = 0;
-  const bool c = siddon_setup(g, e, w);
-  if (c)
-  {
-    int* co = coords + i * cap;
-    double* le = lengths + i * cap;
-    if (!siddon_walk(g, w, [&](int v, double len) {
-          if (k < cap)
-          {
-            co[k] = v;
-            le[k] = len;
-          }
-          ++k;
-        }))
+    for (int k = 0; k < 6; ++k)
     {
-      flag(check, kCheckWalkGuard);
+      e[k] = ends[6 * i + k];
     }
+    go = siddon_setup(g, e, w);
   }
-  counts[i] = k;
-  crosses[i] = c ? 1 : 0;
+  dump_path(g, w, go, i, cap, coords, lengths, counts, crosses, valid, check);
 }
 
 __global__ void k_lor_paths(Grid g, Sino s, Tables t, long long n, const long long* __restrict__ bins,
@@ -186,42 +214,22 @@ __global__ void k_lor_paths(Grid g, Sino s, Tables t, long long n, const long lo
                             int* check)
 {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= n)
+  const bool valid = i < n;
+  Walk w{};
+  bool go = false;
+  if (valid)
   {
-    return;
-  }
-  // bins are flat file-order indices: enumerate with one subset.
-  const long long b = bins[i];
-  if (b < 0 || b >= s.n_enum)
-  {
-    counts[i] = 0;
-    crosses[i] = 0;
-    return;
-  }
-  const Lor l = decode_bin(s, (int)b);
-  double e[6];
-  lor_ends(s, t, l, e);
-  Walk w;
-  int k = 0;
-  const bool c = siddon_setup(g, e, w);
-  if (c)
-  {
-    int* co = coords + i * cap;
-    double* le = lengths + i * cap;
-    if (!siddon_walk(g, w, [&](int v, double len) {
-          if (k < cap)
-          {
-            co[k] = v;
-            le[k] = len;
-          }
-          ++k;
-        }))
+    // bins are flat file-order indices: enumerated with one subset
+    const long long b = bins[i];
+    if (b >= 0 && b < s.n_enum)
     {
-      flag(check, kCheckWalkGuard);
+      const Lor l = decode_bin(s, (int)b);
+      double e[6];
+      lor_ends(s, t, l, e);
+      go = siddon_setup(g, e, w);
     }
   }
-  counts[i] = k;
-  crosses[i] = c ? 1 : 0;
+  dump_path(g, w, go, i, cap, coords, lengths, counts, crosses, valid, check);
 }
 
 unsigned blocks_for(long long n, int block)

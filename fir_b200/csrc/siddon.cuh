@@ -6,6 +6,11 @@
 // tie tolerance are FIR's, and the loop visits and emits exactly the voxels
 // FIR's computePath emits, with the same lengths.  The voxel index lists are
 // therefore bit-identical to FIR's.
+//
+// The loop is warp-synchronous: every lane of a warp executes each step
+// together (a vote decides whether any lane still has a step to take), so a
+// warp's 32 LORs advance in lockstep even across the two traversals of the
+// fused OSEM kernel.
 #pragma once
 
 #include <cstdint>
@@ -14,11 +19,13 @@ namespace fir
 {
 constexpr double kEps = 0.00001;   // macros.h:8
 constexpr int kMaxSegments = 255;  // 2*128-1 segments: up to 128 rings at span 1
+constexpr unsigned kFullWarp = 0xffffffffu;
 
 // Volume grid as the traversal sees it (Siddon.cc:20-63).
 struct Grid
 {
   int nx, ny, nz, nxy;
+  int guard;       // bound on traversal steps: planes crossed in all dimensions + margin
   double ext[3];   // step sizes: FIR's int-truncated extents, or the real ones
   double low[3];   // border planes: x,y = offset - voxel/2, z = offset - depth/2
   double high[3];  // low + n * voxel (real voxel extents, as in FIR)
@@ -166,13 +173,17 @@ __device__ __forceinline__ void lor_ends(const Sino& s, const Tables& t, const L
   e[5] = __ldg(t.z + a2);
 }
 
-// State of one path between two plane crossings.
+// State of one path.  The voxel is tracked as its linear index plus, per
+// dimension, the number of further advances that keep the index inside the
+// volume: FIR's checkIndices (Siddon.cc:394-404) holds exactly while all
+// three counts are non-negative, because each index moves monotonically.
 struct Walk
 {
   double a[3];   // alpha of the next plane crossing in each dimension
   double da[3];  // alpha between neighbouring planes
-  int pos[3];    // current voxel
-  int dir[3];
+  int left[3];   // advances left before the index leaves the volume
+  int step[3];   // change of the linear index per advance
+  int c;         // linear index of the current voxel
   double amin, amax, d12;
 };
 
@@ -182,6 +193,7 @@ struct Walk
 __device__ __forceinline__ bool siddon_setup(const Grid& g, const double e[6], Walk& w)
 {
   double diff[3], smin[3], smax[3], snext[3];
+  int dir[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d)
   {
@@ -192,13 +204,13 @@ __device__ __forceinline__ bool siddon_setup(const Grid& g, const double e[6], W
     {
       if (df > 0)
       {
-        w.dir[d] = 1;
+        dir[d] = 1;
         smin[d] = ddiv(dsub(lo, c1), df);
         smax[d] = ddiv(dsub(hi, c1), df);
       }
       else
       {
-        w.dir[d] = -1;
+        dir[d] = -1;
         smin[d] = ddiv(dsub(hi, c1), df);
         smax[d] = ddiv(dsub(lo, c1), df);
       }
@@ -211,7 +223,7 @@ __device__ __forceinline__ bool siddon_setup(const Grid& g, const double e[6], W
         return false;
       }
       df = kEps;
-      w.dir[d] = -1;
+      dir[d] = -1;
       smin[d] = 0.0;
       smax[d] = 1.0;
       snext[d] = 1.0;
@@ -229,68 +241,77 @@ __device__ __forceinline__ bool siddon_setup(const Grid& g, const double e[6], W
   {
     return false;
   }
-  const int nm1[3] = {g.nx - 1, g.ny - 1, g.nz - 1};
+  const int n[3] = {g.nx, g.ny, g.nz};
+  const int stride[3] = {1, g.nx, g.nxy};
 #pragma unroll
   for (int d = 0; d < 3; ++d)
   {
     w.da[d] = ddiv(g.ext[d], fabs(diff[d]));
   }
   w.d12 = __dsqrt_rn(dadd(dadd(dmul(diff[0], diff[0]), dmul(diff[1], diff[1])), dmul(diff[2], diff[2])));
+  w.c = 0;
 #pragma unroll
   for (int d = 0; d < 3; ++d)
   {
     int ind = __double2int_rz(ddiv(dsub(dadd(e[d], dmul(diff[d], w.amin)), g.low[d]), g.ext[d]));
-    ind = ind < nm1[d] ? ind : nm1[d];
-    w.pos[d] = ind > 0 ? ind : 0;
+    ind = ind < n[d] - 1 ? ind : n[d] - 1;
+    ind = ind > 0 ? ind : 0;
     double al = snext[d];
     if (al < 1.0)
     {
-      al = ddiv(dsub(dadd(g.low[d], dmul(g.ext[d], (double)w.pos[d])), e[d]), diff[d]);
+      al = ddiv(dsub(dadd(g.low[d], dmul(g.ext[d], (double)ind)), e[d]), diff[d]);
     }
-    if (w.dir[d] > 0)
+    if (dir[d] > 0)
     {
       al = dadd(al, w.da[d]);
     }
     w.a[d] = al;
+    w.left[d] = dir[d] > 0 ? n[d] - 1 - ind : ind;
+    w.step[d] = dir[d] * stride[d];
+    w.c += ind * stride[d];
   }
   return true;
 }
 
-// The computePath loop (Siddon.cc:207-252).  emit(linearIndex, length) is
-// called for every element FIR would store, in FIR's order.  Returns false
-// if the iteration bound (a path can cross at most nx+ny+nz+3 planes) was
-// hit, which only non-finite input can cause.
+// The computePath loop (Siddon.cc:207-252), warp-synchronous.  Every lane of
+// the warp must call it (lanes with nothing to trace pass go = false).
+// emit(inside, linearIndex, length) is called at every step of an active
+// lane; inside is FIR's checkIndices, i.e. whether FIR stores the element.
+// Returns false for a lane that hit the step bound, which only non-finite
+// input can cause.
 template<class Emit>
-__device__ __forceinline__ bool siddon_walk(const Grid& g, Walk w, Emit&& emit)
+__device__ __forceinline__ bool siddon_walk(const Grid& g, Walk w, bool go, Emit&& emit)
 {
   double prev = w.amin;
-  int guard = g.nx + g.ny + g.nz + 4;
-  while (prev < w.amax)
+  int guard = g.guard;
+  bool active = go && prev < w.amax;
+  while (__any_sync(kFullWarp, active))
   {
-    if (--guard < 0)
+    if (active)
     {
-      return false;
-    }
-    // MIN(alphaMax, MIN(ax, MIN(ay, az))); fmin differs from the macro only
-    // in the sign of a zero result, which no emitted value depends on.
-    const double next = fmin(w.amax, fmin(w.a[0], fmin(w.a[1], w.a[2])));
-    if ((unsigned)w.pos[0] < (unsigned)g.nx && (unsigned)w.pos[1] < (unsigned)g.ny &&
-        (unsigned)w.pos[2] < (unsigned)g.nz)
-    {
-      emit(w.pos[0] + w.pos[1] * g.nx + w.pos[2] * g.nxy, dmul(dsub(next, prev), w.d12));
-    }
+      // MIN(alphaMax, MIN(ax, MIN(ay, az))); fmin differs from the macro
+      // only in the sign of a zero result, which no emitted value depends on.
+      const double next = fmin(fmin(w.a[0], w.a[1]), fmin(w.a[2], w.amax));
+      const bool inside = (w.left[0] | w.left[1] | w.left[2]) >= 0;
+      emit(inside, w.c, dmul(dsub(next, prev), w.d12));
 #pragma unroll
-    for (int d = 0; d < 3; ++d)
-    {
-      if (fabs(dsub(w.a[d], next)) < kEps)
+      for (int d = 0; d < 3; ++d)
       {
-        w.a[d] = dadd(w.a[d], w.da[d]);
-        w.pos[d] += w.dir[d];
+        // a >= next, so |a - next| < EPS is a - next < EPS (updateDim, Siddon.cc:379-392)
+        if (dsub(w.a[d], next) < kEps)
+        {
+          w.a[d] = dadd(w.a[d], w.da[d]);
+          w.c += w.step[d];
+          w.left[d] -= 1;
+        }
       }
+      prev = next;
+      --guard;
+      active = prev < w.amax && guard > 0;
     }
-    prev = next;
   }
-  return true;
+  // a lane stopped by the bound still has prev < amax
+  return !go || !(prev < w.amax);
 }
 
 // VolData::computeLineIntegral accumulation step (VolData.cc:362-368): the
