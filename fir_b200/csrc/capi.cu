@@ -479,7 +479,7 @@ struct fir_ctx
   DevBuf check;     // device check word
   int* check_host = nullptr;  // pinned mirror
 
-  DevBuf bp, conv1, conv2, conv_copy, mu;
+  DevBuf bp, conv1, conv2, conv_copy, mu, wide;
   std::vector<DevBuf> staging;
 
   // projector-kernel timing (FIR_OPT_TIMING)
@@ -557,6 +557,15 @@ void drain_timing(fir_ctx& c)
     c.ev_pool.push_back(p.second);
   }
   c.ev_pending.clear();
+}
+
+// Double copy of a float image in context scratch, for the projector gathers.
+const double* widen(fir_ctx& c, const float* img, long long n)
+{
+  double* d = static_cast<double*>(c.wide.ensure((size_t)n * sizeof(double)));
+  launch_widen(n, img, d, cfg_of(c));
+  after_launch(c);
+  return d;
 }
 
 Tables tables_of(fir_ctx& c, const ProjInfo& p)
@@ -877,7 +886,8 @@ void osem_subiteration_device(fir_ctx& c, const ProjInfo& p, const Tables& t, co
   float* bp = static_cast<float*>(c.bp.ensure((size_t)v.nvox * sizeof(float)));
   cuda_ok(cudaMemsetAsync(bp, 0, (size_t)v.nvox * sizeof(float), c.stream), "cudaMemsetAsync");
   const Sino s = sino_of(p, prm->n_subsets, subset);
-  timed_launch(c, [&] { launch_osem_subset(g, s, t, img, sino, bias, bp, c.skip_zero != 0, cfg_of(c)); });
+  const double* wimg = widen(c, img, v.nvox);
+  timed_launch(c, [&] { launch_osem_subset(g, s, t, wimg, sino, bias, bp, c.skip_zero != 0, cfg_of(c)); });
   launch_em_update(v.nvox, img, bp, sens_frame, cfg_of(c));
   after_launch(c);
   const bool conv = prm->convolution_interval > 0 && prm->fwhm_xyz[0] > 0.0 && prm->fwhm_xyz[1] > 0.0 &&
@@ -995,7 +1005,7 @@ fir_status fir_ctx_destroy(fir_ctx* c)
     }
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    for (DevBuf* b : {&c->xy, &c->z, &c->check, &c->bp, &c->conv1, &c->conv2, &c->conv_copy, &c->mu})
+    for (DevBuf* b : {&c->xy, &c->z, &c->check, &c->bp, &c->conv1, &c->conv2, &c->conv_copy, &c->mu, &c->wide})
     {
       b->release();
     }
@@ -1152,7 +1162,8 @@ fir_status fir_forward(fir_ctx* ctx, const fir_vol_desc* vol, const float* img, 
     const float* dimg = st.in(img, v.nvox);
     float* dsino = st.out(sino, p.g.n_bins);
     const Sino s = sino_of(p, 1, 0);
-    timed_launch(c, [&] { launch_forward(g, s, t, dimg, dsino, FwdEpilogue::None, cfg_of(c)); });
+    const double* wimg = widen(c, dimg, v.nvox);
+    timed_launch(c, [&] { launch_forward(g, s, t, wimg, dsino, FwdEpilogue::None, cfg_of(c)); });
     finish(c, st);
   });
 }
@@ -1170,7 +1181,8 @@ fir_status fir_forward_exp(fir_ctx* ctx, const fir_vol_desc* vol, const float* m
     const float* dmu = st.in(mu, v.nvox);
     float* dacf = st.out(acf, p.g.n_bins);
     const Sino s = sino_of(p, 1, 0);
-    timed_launch(c, [&] { launch_forward(g, s, t, dmu, dacf, FwdEpilogue::Exp, cfg_of(c)); });
+    const double* wmu = widen(c, dmu, v.nvox);
+    timed_launch(c, [&] { launch_forward(g, s, t, wmu, dacf, FwdEpilogue::Exp, cfg_of(c)); });
     finish(c, st);
   });
 }

@@ -36,6 +36,15 @@ __global__ void k_em_update(long long n, float* __restrict__ img, float* __restr
   bp[i] = q;
 }
 
+__global__ void k_widen(long long n, const float* __restrict__ in, double* __restrict__ out)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n)
+  {
+    out[i] = (double)in[i];
+  }
+}
+
 // One pass of operations::convolve (operations.cc:84-156): sum and weight
 // norm over the in-bounds taps, accumulated in float in tap order, then
 // sum / norm.
@@ -180,6 +189,14 @@ void launch_em_update(long long n, float* img, float* bp, const float* sens, con
   if (n > 0)
   {
     k_em_update<<<blocks_for(n), kBlock, 0, cfg.stream>>>(n, img, bp, sens);
+  }
+}
+
+void launch_widen(long long n, const float* in, double* out, const LaunchCfg& cfg)
+{
+  if (n > 0)
+  {
+    k_widen<<<blocks_for(n), kBlock, 0, cfg.stream>>>(n, in, out);
   }
 }
 

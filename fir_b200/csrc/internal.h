@@ -28,11 +28,11 @@ struct LaunchCfg
 };
 
 // projector.cu
-void launch_forward(const Grid& g, const Sino& s, const Tables& t, const float* img, float* sino,
+void launch_forward(const Grid& g, const Sino& s, const Tables& t, const double* img, float* sino,
                     FwdEpilogue ep, const LaunchCfg& cfg);
 void launch_backward(const Grid& g, const Sino& s, const Tables& t, const float* sino, float* img,
                      bool skip_zero, const LaunchCfg& cfg);
-void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const float* img,
+void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const double* img,
                         const float* sino, const float* bias, float* bp, bool skip_zero,
                         const LaunchCfg& cfg);
 void launch_siddon_paths(const Grid& g, long long n, const double* ends, int cap, int* coords,
@@ -49,6 +49,8 @@ struct Taps
   float w[2 * kMaxHalfTaps + 1];
 };
 void launch_em_update(long long n, float* img, float* bp, const float* sens, const LaunchCfg& cfg);
+// Exact widening of a float image to double for the projector gathers.
+void launch_widen(long long n, const float* in, double* out, const LaunchCfg& cfg);
 // One separable pass of operations::convolve along axis (0=x, 1=y, 2=z).
 void launch_conv_pass(int nx, int ny, int nz, int axis, const Taps& taps, const float* in, float* out,
                       const LaunchCfg& cfg);

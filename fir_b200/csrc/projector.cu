@@ -6,11 +6,12 @@
 // bins of one view and axial plane, so a warp holds a bundle of 32 nearly
 // parallel, adjacent LORs: their traversals have near-equal trip counts and
 // touch neighbouring voxels, which keeps the gathers and scatters of a warp
-// step within a few L1/L2 sectors.  The traversal is warp-synchronous (see
-// siddon.cuh), so no lane leaves its warp; kernels therefore never return
-// early: lanes without work pass go = false to the traversal.  Paths are
-// recomputed on the fly (no LOR cache, no stored path) and the image (tens of
-// MB) stays resident in the 126 MB L2.
+// step within a few L1/L2 sectors.  Kernels never return early: every lane
+// reaches every traversal (lanes without work pass go = false), so warps
+// stay converged and __syncwarp() between two traversals is safe.  Paths are
+// recomputed on the fly (no LOR cache, no stored path).  The image is
+// gathered from a double-precision copy (exact widening of the float image,
+// made once per call), which stays resident in the 126 MB L2.
 #include "internal.h"
 
 namespace fir
@@ -30,7 +31,7 @@ __device__ __forceinline__ void flag(int* check, int bit)
 // ProjData::exponential (ProjData.cc:514-539).
 template<FwdEpilogue EP>
 __global__ void __launch_bounds__(256) k_forward(Grid g, Sino s, Tables t,
-                                                 const float* __restrict__ img,
+                                                 const double* __restrict__ img,
                                                  float* __restrict__ sino, int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(256) k_backward(Grid g, Sino s, Tables t,
 // same path.  The path is traversed twice from the same saved setup, so both
 // traversals visit identical voxels with identical lengths.
 __global__ void __launch_bounds__(256) k_osem_subset(Grid g, Sino s, Tables t,
-                                                     const float* __restrict__ img,
+                                                     const double* __restrict__ img,
                                                      const float* __restrict__ sino,
                                                      const float* __restrict__ bias, float* bp,
                                                      int skip_zero, int* check)
@@ -141,6 +142,7 @@ __global__ void __launch_bounds__(256) k_osem_subset(Grid g, Sino s, Tables t,
       line = accumulate(line, len, __ldg(img + c));
     }
   });
+  __syncwarp();
   if (valid && bias != nullptr)
   {
     line = __fadd_rn(line, __ldg(bias + l.bin));
@@ -238,7 +240,7 @@ unsigned blocks_for(long long n, int block)
 }
 }  // namespace
 
-void launch_forward(const Grid& g, const Sino& s, const Tables& t, const float* img, float* sino,
+void launch_forward(const Grid& g, const Sino& s, const Tables& t, const double* img, float* sino,
                     FwdEpilogue ep, const LaunchCfg& cfg)
 {
   if (s.n_enum == 0)
@@ -267,7 +269,7 @@ void launch_backward(const Grid& g, const Sino& s, const Tables& t, const float*
     g, s, t, sino, img, skip_zero ? 1 : 0, cfg.check);
 }
 
-void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const float* img,
+void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const double* img,
                         const float* sino, const float* bias, float* bp, bool skip_zero,
                         const LaunchCfg& cfg)
 {

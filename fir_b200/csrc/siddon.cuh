@@ -7,10 +7,10 @@
 // FIR's computePath emits, with the same lengths.  The voxel index lists are
 // therefore bit-identical to FIR's.
 //
-// The loop is warp-synchronous: every lane of a warp executes each step
-// together (a vote decides whether any lane still has a step to take), so a
-// warp's 32 LORs advance in lockstep even across the two traversals of the
-// fused OSEM kernel.
+// Kernels call the traversal from every lane (lanes without a LOR pass
+// go = false) and never return before it, so a warp's 32 LORs step through
+// their loops together; between two traversals of one lane the kernel
+// re-converges the warp with __syncwarp().
 #pragma once
 
 #include <cstdint>
@@ -19,7 +19,6 @@ namespace fir
 {
 constexpr double kEps = 0.00001;   // macros.h:8
 constexpr int kMaxSegments = 255;  // 2*128-1 segments: up to 128 rings at span 1
-constexpr unsigned kFullWarp = 0xffffffffu;
 
 // Volume grid as the traversal sees it (Siddon.cc:20-63).
 struct Grid
@@ -273,10 +272,15 @@ __device__ __forceinline__ bool siddon_setup(const Grid& g, const double e[6], W
   return true;
 }
 
-// The computePath loop (Siddon.cc:207-252), warp-synchronous.  Every lane of
-// the warp must call it (lanes with nothing to trace pass go = false).
-// emit(inside, linearIndex, length) is called at every step of an active
-// lane; inside is FIR's checkIndices, i.e. whether FIR stores the element.
+// MIN macro of macros.h:4 on doubles (a compare and a select; cheaper on the
+// GPU than fmin, which must also order NaNs and signed zeros).
+__device__ __forceinline__ double min_of(double a, double b) { return a < b ? a : b; }
+
+// The computePath loop (Siddon.cc:207-252).  emit(inside, linearIndex,
+// length) is called at every step; inside is FIR's checkIndices, i.e.
+// whether FIR stores the element.  Lanes with nothing to trace pass
+// go = false.  A kernel that traverses twice per lane must call __syncwarp()
+// between the traversals so that the warp enters the second one converged.
 // Returns false for a lane that hit the step bound, which only non-finite
 // input can cause.
 template<class Emit>
@@ -285,30 +289,27 @@ __device__ __forceinline__ bool siddon_walk(const Grid& g, Walk w, bool go, Emit
   double prev = w.amin;
   int guard = g.guard;
   bool active = go && prev < w.amax;
-  while (__any_sync(kFullWarp, active))
+  while (active)
   {
-    if (active)
-    {
-      // MIN(alphaMax, MIN(ax, MIN(ay, az))); fmin differs from the macro
-      // only in the sign of a zero result, which no emitted value depends on.
-      const double next = fmin(fmin(w.a[0], w.a[1]), fmin(w.a[2], w.amax));
-      const bool inside = (w.left[0] | w.left[1] | w.left[2]) >= 0;
-      emit(inside, w.c, dmul(dsub(next, prev), w.d12));
+    // MIN(alphaMax, MIN(ax, MIN(ay, az))) in FIR's order, which also fixes
+    // which operand wins when an alpha is NaN (non-finite end points).
+    const double next = min_of(w.amax, min_of(w.a[0], min_of(w.a[1], w.a[2])));
+    const bool inside = (w.left[0] | w.left[1] | w.left[2]) >= 0;
+    emit(inside, w.c, dmul(dsub(next, prev), w.d12));
 #pragma unroll
-      for (int d = 0; d < 3; ++d)
+    for (int d = 0; d < 3; ++d)
+    {
+      // a >= next, so |a - next| < EPS is a - next < EPS (updateDim, Siddon.cc:379-392)
+      if (dsub(w.a[d], next) < kEps)
       {
-        // a >= next, so |a - next| < EPS is a - next < EPS (updateDim, Siddon.cc:379-392)
-        if (dsub(w.a[d], next) < kEps)
-        {
-          w.a[d] = dadd(w.a[d], w.da[d]);
-          w.c += w.step[d];
-          w.left[d] -= 1;
-        }
+        w.a[d] = dadd(w.a[d], w.da[d]);
+        w.c += w.step[d];
+        w.left[d] -= 1;
       }
-      prev = next;
-      --guard;
-      active = prev < w.amax && guard > 0;
     }
+    prev = next;
+    --guard;
+    active = prev < w.amax && guard > 0;
   }
   // a lane stopped by the bound still has prev < amax
   return !go || !(prev < w.amax);
@@ -316,9 +317,11 @@ __device__ __forceinline__ bool siddon_walk(const Grid& g, Walk w, bool go, Emit
 
 // VolData::computeLineIntegral accumulation step (VolData.cc:362-368): the
 // float running sum is widened, the double product added, the sum rounded.
-__device__ __forceinline__ float accumulate(float line, double length, float value)
+// `value` is the voxel widened to double: the projectors gather from a
+// double copy of the float image (exact), which saves a conversion per step.
+__device__ __forceinline__ float accumulate(float line, double length, double value)
 {
-  return __double2float_rn(dadd((double)line, dmul(length, (double)value)));
+  return __double2float_rn(dadd((double)line, dmul(length, value)));
 }
 
 }  // namespace fir
