@@ -110,6 +110,10 @@ _SIGS = {
                                         C.c_int, C.c_int]),
     "fir_osem": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.c_void_p, C.c_void_p, C.POINTER(VolDesc),
                            C.c_void_p, C.c_void_p, C.POINTER(OsemParamsDesc), C.c_void_p, C.c_void_p]),
+    "fir_osem_subiteration_noalloc": (C.c_int, [C.POINTER(ProjDesc), C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_void_p, C.POINTER(VolDesc), C.c_void_p, C.c_void_p,
+                                                C.POINTER(OsemParamsDesc), C.c_int, C.c_int, C.c_int,
+                                                C.c_void_p]),
     "fir_em_update": (C.c_int, [C.c_void_p, C.POINTER(VolDesc), C.c_void_p, C.c_void_p, C.c_void_p]),
     "fir_convolve": (C.c_int, [C.c_void_p, C.POINTER(VolDesc), C.c_void_p, C.POINTER(C.c_float), C.c_float]),
     "fir_cut_circle": (C.c_int, [C.c_void_p, C.POINTER(VolDesc), C.c_void_p, C.c_float]),

@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -1464,3 +1465,146 @@ fir_status fir_lor_paths(fir_ctx* ctx, const fir_proj_desc* proj, const fir_vol_
 }
 
 }  // extern "C"
+
+// ====================================== OSEM sub-iteration without allocation
+//
+// fir_osem_subiteration_noalloc runs the same kernels as
+// fir_osem_subiteration, but takes its scratch memory (backprojection
+// accumulator, widened image, filter passes, pre-filter copy) from the
+// file-scope array below instead of from a context, and touches no host
+// memory, so it never allocates.  The array's device address is looked up
+// once per device with cudaGetSymbolAddress; the name itself is only a host
+// stand-in and is never passed to a kernel.
+
+namespace
+{
+constexpr long long kNoAllocMaxVoxels = 1LL << 20;
+// per voxel: accumulator (float) + widened image (double) + two filter
+// passes (float) + pre-filter copy (float)
+constexpr size_t kNoAllocBytesPerVoxel = 4 + 8 + 4 + 4 + 4;
+constexpr size_t kNoAllocScratchBytes = (size_t)kNoAllocMaxVoxels * kNoAllocBytesPerVoxel;
+constexpr int kNoAllocMaxDevices = 64;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace
+{
+std::mutex g_noalloc_mutex;
+void* g_noalloc_address[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device (set-up on the
+// first call per device).
+unsigned char* noalloc_scratch()
+{
+  int device = 0;
+  cuda_ok(cudaGetDevice(&device), "cudaGetDevice");
+  if (device < 0 || device >= kNoAllocMaxDevices)
+  {
+    fail(FIR_ERR_NOT_SUPPORTED, "device ordinal ", device, " beyond ", kNoAllocMaxDevices);
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_address[device] == nullptr)
+  {
+    void* p = nullptr;
+    cuda_ok(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
+    g_noalloc_address[device] = p;
+  }
+  return static_cast<unsigned char*>(g_noalloc_address[device]);
+}
+
+void require_device(const void* p, const char* what)
+{
+  if (p != nullptr && !is_device_ptr(p))
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, what, " must be device memory for the no-allocation entry point");
+  }
+}
+}  // namespace
+
+extern "C" fir_status fir_osem_subiteration_noalloc(const fir_proj_desc* proj, const double* crystal_xy,
+                                                    const double* slice_z, const float* sino, const float* bias,
+                                                    const fir_vol_desc* vol, float* img, const float* sens_frame,
+                                                    const fir_osem_params* params, int subset, int subiter,
+                                                    int geometry, void* stream)
+{
+  return guarded([&] {
+    const ProjInfo p = check_proj(proj);
+    check_osem_params(params, p);
+    if (subset < 0 || subset >= params->n_subsets)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "subset ", subset, " out of range [0, ", params->n_subsets, ")");
+    }
+    const VolInfo v = check_vol(vol);
+    check_frames(v, 1);
+    if (v.nvox > kNoAllocMaxVoxels)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "volume of ", v.nvox, " voxels exceeds the no-allocation limit of ",
+           kNoAllocMaxVoxels, " voxels");
+    }
+    if (geometry != FIR_GEOMETRY_REFERENCE && geometry != FIR_GEOMETRY_EXACT)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "unknown geometry mode ", geometry);
+    }
+    if (crystal_xy == nullptr || slice_z == nullptr || sino == nullptr || img == nullptr || sens_frame == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "tables, sinogram, image and sensitivity must not be NULL");
+    }
+    require_device(crystal_xy, "crystal_xy");
+    require_device(slice_z, "slice_z");
+    require_device(sino, "sino");
+    require_device(bias, "bias");
+    require_device(img, "img");
+    require_device(sens_frame, "sens_frame");
+
+    // geometry as a context in the requested mode would build it
+    fir_ctx geo;
+    geo.geometry = geometry;
+    const Grid g = grid_of(geo, v);
+    const Sino s = sino_of(p, params->n_subsets, subset);
+    const Tables t{reinterpret_cast<const double2*>(crystal_xy), slice_z};
+
+    unsigned char* base = noalloc_scratch();
+    const size_t n = (size_t)kNoAllocMaxVoxels;
+    float* bp = reinterpret_cast<float*>(base);
+    double* wide = reinterpret_cast<double*>(base + 4 * n);
+    float* t1 = reinterpret_cast<float*>(base + 12 * n);
+    float* t2 = reinterpret_cast<float*>(base + 16 * n);
+    float* copy = reinterpret_cast<float*>(base + 20 * n);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const LaunchCfg cfg{128, st, nullptr};
+
+    // the accumulator keeps the previous call's sums: clear it
+    cuda_ok(cudaMemsetAsync(bp, 0, (size_t)v.nvox * sizeof(float), st), "cudaMemsetAsync");
+    launch_widen(v.nvox, img, wide, cfg);
+    launch_osem_subset(g, s, t, wide, sino, bias, bp, false, cfg);
+    launch_em_update(v.nvox, img, bp, sens_frame, cfg);
+    const float* fwhm = params->fwhm_xyz;
+    const bool conv = params->convolution_interval > 0 && fwhm[0] > 0.0 && fwhm[1] > 0.0 && fwhm[2] > 0.0;
+    if (conv && subiter % params->convolution_interval == 0)
+    {
+      const Taps tx = gauss_taps(fwhm[0], v.d.voxel_x, false);
+      const Taps ty = gauss_taps(fwhm[1], v.d.voxel_y, false);
+      const Taps tz = gauss_taps(fwhm[2], v.d.voxel_z, true);
+      const float cut = params->cut_radius;
+      if (cut > 0.0f)
+      {
+        cuda_ok(cudaMemcpyAsync(copy, img, (size_t)v.nvox * sizeof(float), cudaMemcpyDeviceToDevice, st),
+                "cudaMemcpyAsync");
+      }
+      launch_conv_pass(v.d.nx, v.d.ny, v.d.nz, 0, tx, img, t1, cfg);
+      launch_conv_pass(v.d.nx, v.d.ny, v.d.nz, 1, ty, t1, t2, cfg);
+      launch_conv_pass(v.d.nx, v.d.ny, v.d.nz, 2, tz, t2, img, cfg);
+      if (cut > 0.0f)
+      {
+        launch_conv_restore(v.d.nx, v.d.ny, v.d.nz, v.d.voxel_x, v.d.voxel_y, cut, fwhm[0] > fwhm[1] ? fwhm[0] : fwhm[1],
+                            copy, img, cfg);
+      }
+    }
+    if (params->cut_radius > 0.0f)
+    {
+      launch_cut_circle(v.d.nx, v.d.ny, v.d.nz, v.d.voxel_x, v.d.voxel_y, params->cut_radius, img, cfg);
+    }
+    cuda_ok(cudaGetLastError(), "kernel launch");
+  });
+}

@@ -219,6 +219,35 @@ fir_status fir_osem_subiteration(fir_ctx* ctx, const fir_proj_desc* proj, const 
                                  const float* sens_frame, const fir_osem_params* params,
                                  int subset, int subiter);
 
+/* The same OSEM sub-iteration for callers that cannot allocate GPU memory
+ * once they are running: reconstruction services that reserve their whole
+ * device-memory budget at start-up and forbid later allocations (an
+ * allocation can fail or stall when the budget is spent or fragmented), and
+ * hosts whose GPU memory belongs to their own pool allocator, where an
+ * allocation by the library would fail or force the pool to give memory
+ * back.  This entry point has no counterpart in FIR.
+ *
+ * It allocates nothing and needs no context: every pointer (sinogram, bias,
+ * image, sensitivity frame, and the scanner tables crystal_xy = 2 *
+ * n_crystals_per_ring doubles and slice_z = 2 * n_rings - 1 doubles, as
+ * fir_scanner_tables returns them) must be device memory, and the work is
+ * enqueued on `stream` (a cudaStream_t) without waiting.  Its scratch memory
+ * is one array in the library's static device memory, 24 MiB on every GPU
+ * that loads the library, held until the process exits; volumes of more than
+ * 1048576 voxels (1 << 20) are rejected with FIR_ERR_INVALID_ARGUMENT.  The
+ * first call on each device looks up the array's address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls on a device share the one array, so calls that can overlap on
+ * the GPU (different streams, no ordering between them) race and corrupt
+ * each other; order them on one stream.  The accumulator is cleared by each
+ * call.  geometry is FIR_GEOMETRY_REFERENCE or FIR_GEOMETRY_EXACT.
+ * Device-side checks of non-finite input are not reported by this call. */
+fir_status fir_osem_subiteration_noalloc(const fir_proj_desc* proj, const double* crystal_xy,
+                                         const double* slice_z, const float* sino, const float* bias,
+                                         const fir_vol_desc* vol, float* img, const float* sens_frame,
+                                         const fir_osem_params* params, int subset, int subiter,
+                                         int geometry, void* stream);
+
 /* Called by fir_osem after sub-iteration `subiter` when params->save_interval
  * asks for an intermediate image; img is a host copy (nx*ny*nz floats). */
 typedef void (*fir_osem_save_fn)(void* user, int subiter, const float* img);
