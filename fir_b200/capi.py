@@ -114,6 +114,8 @@ _SIGS = {
                                                 C.c_void_p, C.POINTER(VolDesc), C.c_void_p, C.c_void_p,
                                                 C.POINTER(OsemParamsDesc), C.c_int, C.c_int, C.c_int,
                                                 C.c_void_p]),
+    "fir_ratio_backprojection": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.c_void_p, C.c_void_p,
+                                           C.POINTER(VolDesc), C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
     "fir_em_update": (C.c_int, [C.c_void_p, C.POINTER(VolDesc), C.c_void_p, C.c_void_p, C.c_void_p]),
     "fir_convolve": (C.c_int, [C.c_void_p, C.POINTER(VolDesc), C.c_void_p, C.POINTER(C.c_float), C.c_float]),
     "fir_cut_circle": (C.c_int, [C.c_void_p, C.POINTER(VolDesc), C.c_void_p, C.c_float]),
@@ -374,6 +376,15 @@ class Context:
                               C.byref(vol_desc(vol, 1)), _ptr(img, writable=True, n=vol.n_voxels),
                               _ptr(sens, n=vol.n_voxels * params.n_subsets), C.byref(osem_desc(params)),
                               C.cast(cb, C.c_void_p) if cb is not None else None, None))
+
+    def ratio_backprojection(self, proj: ProjSpec, sino, vol: VolSpec, img, bp, n_subsets: int = 1,
+                             subset: int = 0, bias=None) -> None:
+        """bp <- backprojection of sino / (projection of img + bias) over one subset."""
+        self._prep(sino, img, bp, bias)
+        nb = proj_geometry(proj)["n_bins"]
+        _check(lib().fir_ratio_backprojection(self._h, C.byref(proj_desc(proj)), _ptr(sino, n=nb), _ptr(bias, n=nb),
+                                              C.byref(vol_desc(vol, 1)), _ptr(img, n=vol.n_voxels),
+                                              _ptr(bp, writable=True, n=vol.n_voxels), int(n_subsets), int(subset)))
 
     # -- image / sinogram operations
     def em_update(self, vol: VolSpec, img, bp, sens_frame) -> None:

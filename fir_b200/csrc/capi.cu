@@ -1318,6 +1318,38 @@ fir_status fir_osem(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, 
   });
 }
 
+fir_status fir_ratio_backprojection(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const float* bias,
+                                    const fir_vol_desc* vol, const float* img, float* bp, int n_subsets, int subset)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const ProjInfo p = check_proj(proj);
+    check_subsets(p, n_subsets);
+    if (subset < 0 || subset >= n_subsets)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "subset ", subset, " out of range [0, ", n_subsets, ")");
+    }
+    const VolInfo v = check_vol(vol);
+    check_frames(v, 1);
+    const Tables t = tables_of(c, p);
+    const Grid g = grid_of(c, v);
+    if (sino == nullptr || img == nullptr || bp == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "sinogram, image and backprojection must not be NULL");
+    }
+    Stager st(c);
+    const float* dsino = st.in(sino, p.g.n_bins);
+    const float* dbias = st.in(bias, p.g.n_bins);
+    const float* dimg = st.in(img, v.nvox);
+    float* dbp = st.out(bp, v.nvox);
+    cuda_ok(cudaMemsetAsync(dbp, 0, (size_t)v.nvox * sizeof(float), c.stream), "cudaMemsetAsync");
+    const Sino s = sino_of(p, n_subsets, subset);
+    const double* wimg = widen(c, dimg, v.nvox);
+    timed_launch(c, [&] { launch_osem_subset(g, s, t, wimg, dsino, dbias, dbp, c.skip_zero != 0, cfg_of(c)); });
+    finish(c, st);
+  });
+}
+
 fir_status fir_em_update(fir_ctx* ctx, const fir_vol_desc* vol, float* img, float* bp, const float* sens_frame)
 {
   return guarded([&] {

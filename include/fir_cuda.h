@@ -10,6 +10,7 @@
  *   fir_sensitivity        projections::computeSensitivityVol  src_lib/projections.h:20-24, projections.cc:186-197
  *   fir_osem_subiteration  one sub-iteration of reconAlgos::OSEM  src_lib/reconAlgos.cc:119-198
  *   fir_osem               reconAlgos::OSEM                src_lib/reconAlgos.h:29-36, reconAlgos.cc:63-201
+ *   fir_ratio_backprojection  the getLine/ratio/projectLineIntegral loop of OSEM and OSEM_ResoReco  src_lib/reconAlgos.cc:119-158, :273-312
  *   fir_convolve           operations::convolve            src_lib/operations.h:7-10, operations.cc:11-192
  *   fir_cut_circle         operations::cutCircle           src_lib/operations.h:13-15, operations.cc:194-220
  *   fir_apply_mask         operations::applyMask           src_lib/operations.h:19, operations.cc:222-241
@@ -247,6 +248,15 @@ fir_status fir_osem_subiteration_noalloc(const fir_proj_desc* proj, const double
                                          const fir_vol_desc* vol, float* img, const float* sens_frame,
                                          const fir_osem_params* params, int subset, int subiter,
                                          int geometry, void* stream);
+
+/* The projection/ratio/backprojection half of an OSEM sub-iteration alone
+ * (reconAlgos.cc:119-158, also the loop body of OSEM_ResoReco,
+ * reconAlgos.cc:273-312): bp is zeroed, then for every bin of subset
+ * `subset` of n_subsets, line = projection of img (+ bias), and if line >
+ * 1e-5 the ratio sino/line is backprojected into bp.  bias may be NULL. */
+fir_status fir_ratio_backprojection(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino,
+                                    const float* bias, const fir_vol_desc* vol, const float* img,
+                                    float* bp, int n_subsets, int subset);
 
 /* Called by fir_osem after sub-iteration `subiter` when params->save_interval
  * asks for an intermediate image; img is a host copy (nx*ny*nz floats). */

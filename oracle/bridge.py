@@ -24,7 +24,10 @@ from fir_b200.geometry import ProjSpec, ScannerSpec, VolSpec, OSEMParams
 from fir_b200 import interfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
 RESTATED_SO = os.path.join(HERE, "libfir_oracle.so")
+REF_BIN = os.path.join(HERE, "_ref")
+DROPIN_BIN = os.path.join(HERE, "_ref", "dropin")
 REF_SO = os.path.join(HERE, "_ref", "libfirref.so")
 REF_SOURCES = os.environ.get("FIR_REFERENCE_SRC", "/root/reference")
 
@@ -34,10 +37,13 @@ _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 
 
 def build(reference: bool = True) -> None:
-    """Builds the restatement, and the reference when its sources exist."""
+    """Builds the restatement, and the reference (plus FIR's executables
+    compiled against the drop-in layer) when FIR's sources exist."""
     targets = ["restated"]
     if reference and os.path.isdir(os.path.join(REF_SOURCES, "src_lib")):
         targets.append("reference")
+        if os.path.exists(os.path.join(ROOT, "fir_b200", "lib", "libfir.so")):
+            targets.append("dropin")
     subprocess.run(["make", "-s", "-C", HERE, f"REF={REF_SOURCES}", "-j8"] + targets, check=True)
 
 
