@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--det-steps", type=int, default=2,
+                    help="extra sub-iterations timed with deterministic backprojection (0: skip)")
     return ap.parse_args()
 
 
@@ -432,6 +434,37 @@ def main():
         "roofline": roofline,
         "clocks": {k2: v for k2, v in clocks.summary().items() if k2 != "samples"},
     }
+
+    # ---- the same steps with deterministic backprojection (FIR's serial order)
+    if args.det_steps > 0:
+        det = capi.Context(w.scanner, device=local)
+        if w.geometry:
+            det.set_option(capi.FIR_OPT_GEOMETRY, w.geometry)
+        det.set_option(capi.FIR_OPT_BACKPROJ_MODE, capi.FIR_BACKPROJ_DETERMINISTIC)
+        dimg = img.clone()
+        det.osem_subiteration(w.proj, y, w.vol, dimg, sens_frames[k % nsub], prm, k % nsub, k + 1)  # warm
+        k += 1
+        det_ms, det_steps = 0.0, 0
+        for _ in range(args.det_steps):
+            s = k % nsub
+            det_steps += s_fwd[s] + s_bwd(s)
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            det.osem_subiteration(w.proj, y, w.vol, dimg, sens_frames[s], prm, s, k + 1)
+            b.record(stream)
+            torch.cuda.synchronize()
+            det_ms += a.elapsed_time(b)
+            k += 1
+        det.close()
+        result["deterministic"] = {
+            "value": det_steps / (det_ms / 1000.0),
+            "unit": UNIT,
+            "ms_per_step": det_ms / args.det_steps,
+            "steps": args.det_steps,
+            "note": "FIR_BACKPROJ_DETERMINISTIC: contributions sorted per voxel into FIR's serial order "
+                    "(bit-identical to single-threaded FIR)",
+        }
 
     # ---- end to end through the C ABI with host buffers: one OSEM iteration
     if not args.no_e2e and rank == 0:

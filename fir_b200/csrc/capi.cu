@@ -471,6 +471,7 @@ struct fir_ctx
   int backproj = FIR_BACKPROJ_ATOMIC;
   int skip_zero = 0;
   int block = 128;
+  long long det_chunk = 1LL << 28;
   long long launches = 0;
 
   bool have_scanner = false;
@@ -480,7 +481,7 @@ struct fir_ctx
   DevBuf check;     // device check word
   int* check_host = nullptr;  // pinned mirror
 
-  DevBuf bp, conv1, conv2, conv_copy, mu, wide;
+  DevBuf bp, conv1, conv2, conv_copy, mu, wide, det, det_pairs, ratio;
   std::vector<DevBuf> staging;
 
   // projector-kernel timing (FIR_OPT_TIMING)
@@ -558,6 +559,46 @@ void drain_timing(fir_ctx& c)
     c.ev_pool.push_back(p.second);
   }
   c.ev_pending.clear();
+}
+
+// Deterministic-mode backprojection of vals (per bin, or per enumerated LOR
+// when by_enum) into img, FIR's serial order; scratch from the context.
+void det_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, const float* vals, bool by_enum,
+                     float* img, long long nvox)
+{
+  const ScratchFn scratch = [&c](int slot, size_t bytes) -> void* {
+    DevBuf& b = slot == 0 ? c.det : c.det_pairs;
+    try
+    {
+      return b.ensure(bytes);
+    }
+    catch (const Failure&)
+    {
+      return nullptr;
+    }
+  };
+  long long launches = 0;
+  // chunks of at most det_chunk pairs (default 2^28: 8 GiB of keys,
+  // products and sort buffers)
+  cuda_ok(deterministic_backproject(g, s, t, vals, by_enum, img, scratch, c.det_chunk, nvox, cfg_of(c), &launches),
+          "deterministic backprojection");
+  c.launches += launches;
+}
+
+// bp (zeroed by the caller) += backprojection of sino / (projection of the
+// widened image + bias) over the subset of s: the fused kernel, or in
+// deterministic mode the ratio kernel followed by the ordered scatter.
+void ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, const double* wimg,
+                       const float* sino, const float* bias, float* bp, long long nvox)
+{
+  if (c.backproj == FIR_BACKPROJ_DETERMINISTIC)
+  {
+    float* ratio = static_cast<float*>(c.ratio.ensure((size_t)std::max(s.n_enum, 1) * sizeof(float)));
+    timed_launch(c, [&] { launch_ratio(g, s, t, wimg, sino, bias, ratio, cfg_of(c)); });
+    det_backproject(c, g, s, t, ratio, true, bp, nvox);
+    return;
+  }
+  timed_launch(c, [&] { launch_osem_subset(g, s, t, wimg, sino, bias, bp, c.skip_zero != 0, cfg_of(c)); });
 }
 
 // Double copy of a float image in context scratch, for the projector gathers.
@@ -888,7 +929,7 @@ void osem_subiteration_device(fir_ctx& c, const ProjInfo& p, const Tables& t, co
   cuda_ok(cudaMemsetAsync(bp, 0, (size_t)v.nvox * sizeof(float), c.stream), "cudaMemsetAsync");
   const Sino s = sino_of(p, prm->n_subsets, subset);
   const double* wimg = widen(c, img, v.nvox);
-  timed_launch(c, [&] { launch_osem_subset(g, s, t, wimg, sino, bias, bp, c.skip_zero != 0, cfg_of(c)); });
+  ratio_backproject(c, g, s, t, wimg, sino, bias, bp, v.nvox);
   launch_em_update(v.nvox, img, bp, sens_frame, cfg_of(c));
   after_launch(c);
   const bool conv = prm->convolution_interval > 0 && prm->fwhm_xyz[0] > 0.0 && prm->fwhm_xyz[1] > 0.0 &&
@@ -1006,7 +1047,8 @@ fir_status fir_ctx_destroy(fir_ctx* c)
     }
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    for (DevBuf* b : {&c->xy, &c->z, &c->check, &c->bp, &c->conv1, &c->conv2, &c->conv_copy, &c->mu, &c->wide})
+    for (DevBuf* b : {&c->xy, &c->z, &c->check, &c->bp, &c->conv1, &c->conv2, &c->conv_copy, &c->mu, &c->wide,
+                      &c->det, &c->det_pairs, &c->ratio})
     {
       b->release();
     }
@@ -1054,10 +1096,6 @@ fir_status fir_ctx_set_option(fir_ctx* ctx, fir_option opt, int value)
       {
         fail(FIR_ERR_INVALID_ARGUMENT, "unknown backprojection mode ", value);
       }
-      if (value == FIR_BACKPROJ_DETERMINISTIC)
-      {
-        fail(FIR_ERR_NOT_SUPPORTED, "deterministic backprojection is not available in this build");
-      }
       c.backproj = value;
       break;
     case FIR_OPT_SKIP_ZERO_BINS:
@@ -1076,6 +1114,14 @@ fir_status fir_ctx_set_option(fir_ctx* ctx, fir_option opt, int value)
       break;
     case FIR_OPT_TIMING:
       c.timing = value != 0;
+      break;
+    case FIR_OPT_DETERMINISTIC_CHUNK:
+      if (value < 0)
+      {
+        fail(FIR_ERR_INVALID_ARGUMENT, "chunk size must not be negative");
+      }
+      // at most 2^30 pairs per chunk (32 GiB of buffers), the sort's item limit
+      c.det_chunk = value == 0 ? (1LL << 28) : std::min<long long>(value, 1LL << 30);
       break;
     default:
       fail(FIR_ERR_INVALID_ARGUMENT, "unknown option ", (int)opt);
@@ -1119,6 +1165,7 @@ fir_status fir_ctx_get_option(fir_ctx* ctx, fir_option opt, int* value)
     case FIR_OPT_SKIP_ZERO_BINS: *value = c.skip_zero; break;
     case FIR_OPT_BLOCK_SIZE: *value = c.block; break;
     case FIR_OPT_TIMING: *value = c.timing ? 1 : 0; break;
+    case FIR_OPT_DETERMINISTIC_CHUNK: *value = (int)std::min<long long>(c.det_chunk, 0x7fffffff); break;
     default: fail(FIR_ERR_INVALID_ARGUMENT, "unknown option ", (int)opt);
     }
   });
@@ -1210,6 +1257,11 @@ fir_status fir_backward(fir_ctx* ctx, const fir_proj_desc* proj, const float* si
     for (int s = 0; s < n_subsets; ++s)
     {
       const Sino ss = sino_of(p, n_subsets, s);
+      if (c.backproj == FIR_BACKPROJ_DETERMINISTIC)
+      {
+        det_backproject(c, g, ss, t, dsino, false, dimg + (size_t)s * v.nvox, v.nvox);
+        continue;
+      }
       timed_launch(c, [&] {
         launch_backward(g, ss, t, dsino, dimg + (size_t)s * v.nvox, c.skip_zero != 0, cfg_of(c));
       });
@@ -1235,6 +1287,11 @@ fir_status fir_sensitivity(fir_ctx* ctx, const fir_proj_desc* proj, const fir_vo
     for (int s = 0; s < n_subsets; ++s)
     {
       const Sino ss = sino_of(p, n_subsets, s);
+      if (c.backproj == FIR_BACKPROJ_DETERMINISTIC)
+      {
+        det_backproject(c, g, ss, t, nullptr, false, dsens + (size_t)s * v.nvox, v.nvox);
+        continue;
+      }
       timed_launch(c, [&] { launch_backward(g, ss, t, nullptr, dsens + (size_t)s * v.nvox, false, cfg_of(c)); });
     }
     finish(c, st);
@@ -1345,7 +1402,7 @@ fir_status fir_ratio_backprojection(fir_ctx* ctx, const fir_proj_desc* proj, con
     cuda_ok(cudaMemsetAsync(dbp, 0, (size_t)v.nvox * sizeof(float), c.stream), "cudaMemsetAsync");
     const Sino s = sino_of(p, n_subsets, subset);
     const double* wimg = widen(c, dimg, v.nvox);
-    timed_launch(c, [&] { launch_osem_subset(g, s, t, wimg, dsino, dbias, dbp, c.skip_zero != 0, cfg_of(c)); });
+    ratio_backproject(c, g, s, t, wimg, dsino, dbias, dbp, v.nvox);
     finish(c, st);
   });
 }

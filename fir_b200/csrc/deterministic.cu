@@ -1,0 +1,303 @@
+// Deterministic backprojection: FIR's serial summation order, reproduced.
+//
+// FIR adds every contribution to its voxel as voxel = float(double(voxel) +
+// length * value) (VolData.cc:373-385).  With float atomics the result
+// depends on the order in which LORs reach a voxel.  Here every contribution
+// becomes a (key, product) pair: the key is the voxel index in the high bits
+// and the LOR's enumeration index in the low bits.  The enumeration index is
+// FIR's serial loop order (subset, segment, view of the subset, axial plane,
+// tangential bin; LORCache.cc:10-81).  After a radix sort on the key, each
+// voxel's run holds its contributions in that order, and one thread per run
+// accumulates them with FIR's rounding.  The result equals a single-threaded
+// FIR run bit for bit, and is independent of scheduling.
+//
+// Work is chunked over contiguous ranges of LORs; chunks are reduced in
+// order, each run continuing from the voxel's value after the previous
+// chunk, so chunking does not change the order either.
+#include <cub/cub.cuh>
+
+#include <vector>
+
+#include "internal.h"
+
+namespace fir
+{
+namespace
+{
+// Number of elements FIR would store for each enumerated LOR (0 for LORs
+// whose value is exactly 0: their products are 0 and leave every voxel
+// unchanged, +0 + -0 included, since accumulators start at +0).
+__global__ void __launch_bounds__(256) k_count(Grid g, Sino s, Tables t, const float* __restrict__ vals,
+                                               int vals_by_enum, int* counts, int* check)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = i < s.n_enum;
+  Walk w{};
+  bool go = false;
+  if (valid)
+  {
+    const Lor l = decode_bin(s, i);
+    const float v = vals == nullptr ? 1.0f : __ldg(vals + (vals_by_enum ? i : l.bin));
+    if (v != 0.0f)
+    {
+      double e[6];
+      lor_ends(s, t, l, e);
+      go = siddon_setup(g, e, w);
+    }
+  }
+  int k = 0;
+  const bool ok = siddon_walk(g, w, go, [&](bool inside, int, double) { k += inside ? 1 : 0; });
+  if (!ok && check != nullptr)
+  {
+    atomicOr(check, kCheckWalkGuard);
+  }
+  if (valid)
+  {
+    counts[i] = k;
+  }
+}
+
+// Writes the pairs of enumerated LORs [first, last) at their offsets
+// (offsets relative to the chunk start).
+__global__ void __launch_bounds__(256) k_emit(Grid g, Sino s, Tables t, const float* __restrict__ vals,
+                                              int vals_by_enum, int first, int last,
+                                              const long long* __restrict__ offsets, long long base,
+                                              int enum_bits, unsigned long long* keys, double* prods)
+{
+  const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = i < last;
+  Walk w{};
+  bool go = false;
+  double v = 0.0;
+  long long at = 0;
+  if (valid)
+  {
+    const Lor l = decode_bin(s, i);
+    const float fv = vals == nullptr ? 1.0f : __ldg(vals + (vals_by_enum ? i : l.bin));
+    v = (double)fv;
+    at = offsets[i] - base;
+    if (fv != 0.0f)
+    {
+      double e[6];
+      lor_ends(s, t, l, e);
+      go = siddon_setup(g, e, w);
+    }
+  }
+  const unsigned long long lor = (unsigned long long)i;
+  siddon_walk(g, w, go, [&](bool inside, int c, double len) {
+    if (inside)
+    {
+      keys[at] = ((unsigned long long)c << enum_bits) | lor;
+      prods[at] = dmul(len, v);
+      ++at;
+    }
+  });
+}
+
+// One thread per run of equal voxel: FIR's sequential accumulation.
+__global__ void k_reduce_runs(long long n, const unsigned long long* __restrict__ keys,
+                              const double* __restrict__ prods, int enum_bits, float* img)
+{
+  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (j >= n)
+  {
+    return;
+  }
+  const unsigned long long voxel = keys[j] >> enum_bits;
+  if (j > 0 && (keys[j - 1] >> enum_bits) == voxel)
+  {
+    return;
+  }
+  float acc = img[voxel];
+  for (long long k = j; k < n && (keys[k] >> enum_bits) == voxel; ++k)
+  {
+    acc = __double2float_rn(dadd((double)acc, prods[k]));
+  }
+  img[voxel] = acc;
+}
+
+// The ratio of one OSEM sub-iteration per enumerated LOR
+// (reconAlgos.cc:119-158): measured / (projection + bias) when that exceeds
+// 1e-5, else 0.
+__global__ void __launch_bounds__(256) k_ratio(Grid g, Sino s, Tables t, const double* __restrict__ img,
+                                               const float* __restrict__ sino, const float* __restrict__ bias,
+                                               float* ratio, int* check)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = i < s.n_enum;
+  Lor l{};
+  Walk w{};
+  bool go = false;
+  if (valid)
+  {
+    l = decode_bin(s, i);
+    double e[6];
+    lor_ends(s, t, l, e);
+    go = siddon_setup(g, e, w);
+  }
+  float line = 0.0f;
+  const bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
+    if (inside)
+    {
+      line = accumulate(line, len, __ldg(img + c));
+    }
+  });
+  if (!ok && check != nullptr)
+  {
+    atomicOr(check, kCheckWalkGuard);
+  }
+  if (valid)
+  {
+    if (bias != nullptr)
+    {
+      line = __fadd_rn(line, __ldg(bias + l.bin));
+    }
+    ratio[i] = (go && ok && (double)line > kEps) ? __fdiv_rn(__ldg(sino + l.bin), line) : 0.0f;
+  }
+}
+
+int bits_for(long long n)
+{
+  int b = 1;
+  while ((1LL << b) < n)
+  {
+    ++b;
+  }
+  return b;
+}
+
+unsigned blocks_for(long long n, int block)
+{
+  return (unsigned)((n + block - 1) / block);
+}
+}  // namespace
+
+void launch_ratio(const Grid& g, const Sino& s, const Tables& t, const double* img, const float* sino,
+                  const float* bias, float* ratio, const LaunchCfg& cfg)
+{
+  if (s.n_enum > 0)
+  {
+    k_ratio<<<blocks_for(s.n_enum, cfg.block), cfg.block, 0, cfg.stream>>>(g, s, t, img, sino, bias, ratio,
+                                                                          cfg.check);
+  }
+}
+
+namespace
+{
+size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+}  // namespace
+
+cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables& t, const float* vals,
+                                      bool vals_by_enum, float* img, const ScratchFn& scratch,
+                                      long long max_pairs_cap, long long n_vox, const LaunchCfg& cfg,
+                                      long long* launches)
+{
+  const long long n = s.n_enum;
+  if (n == 0)
+  {
+    return cudaSuccess;
+  }
+  // 1. path element count of every LOR and their exclusive prefix sum
+  size_t scan_bytes = 0;
+  cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (const int*)nullptr, (long long*)nullptr,
+                                                (int)n, cfg.stream);
+  if (e != cudaSuccess)
+  {
+    return e;
+  }
+  unsigned char* idx = static_cast<unsigned char*>(scratch(0, round256((size_t)n * 4) + round256((size_t)n * 8) +
+                                                                 round256(scan_bytes)));
+  if (idx == nullptr)
+  {
+    return cudaErrorMemoryAllocation;
+  }
+  int* counts = reinterpret_cast<int*>(idx);
+  long long* offsets = reinterpret_cast<long long*>(idx + round256((size_t)n * 4));
+  void* scan_tmp = idx + round256((size_t)n * 4) + round256((size_t)n * 8);
+  k_count<<<blocks_for(n, cfg.block), cfg.block, 0, cfg.stream>>>(g, s, t, vals, vals_by_enum ? 1 : 0, counts,
+                                                                  cfg.check);
+  e = cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, counts, offsets, (int)n, cfg.stream);
+  std::vector<long long> off((size_t)n + 1);
+  int last_count = 0;
+  if (e == cudaSuccess)
+  {
+    e = cudaMemcpyAsync(off.data(), offsets, (size_t)n * 8, cudaMemcpyDeviceToHost, cfg.stream);
+  }
+  if (e == cudaSuccess)
+  {
+    e = cudaMemcpyAsync(&last_count, counts + n - 1, 4, cudaMemcpyDeviceToHost, cfg.stream);
+  }
+  if (e == cudaSuccess)
+  {
+    e = cudaStreamSynchronize(cfg.stream);
+  }
+  if (e != cudaSuccess)
+  {
+    return e;
+  }
+  off[(size_t)n] = off[(size_t)n - 1] + last_count;
+  *launches += 2;
+  const long long total = off[(size_t)n];
+  if (total == 0)
+  {
+    return cudaGetLastError();
+  }
+
+  // 2. pair buffers for chunks of at most max_pairs (at least one LOR's path)
+  long long max_pairs = total < max_pairs_cap ? total : max_pairs_cap;
+  if (max_pairs < g.guard)
+  {
+    max_pairs = g.guard;
+  }
+  size_t sort_bytes = 0;
+  e = cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const unsigned long long*)nullptr,
+                                      (unsigned long long*)nullptr, (const double*)nullptr, (double*)nullptr,
+                                      (int)max_pairs, 0, 64, cfg.stream);
+  if (e != cudaSuccess)
+  {
+    return e;
+  }
+  const size_t slab = round256((size_t)max_pairs * 8);
+  unsigned char* pb = static_cast<unsigned char*>(scratch(1, 4 * slab + round256(sort_bytes)));
+  if (pb == nullptr)
+  {
+    return cudaErrorMemoryAllocation;
+  }
+  auto* keys_a = reinterpret_cast<unsigned long long*>(pb);
+  auto* keys_b = reinterpret_cast<unsigned long long*>(pb + slab);
+  auto* prods_a = reinterpret_cast<double*>(pb + 2 * slab);
+  auto* prods_b = reinterpret_cast<double*>(pb + 3 * slab);
+  void* sort_tmp = pb + 4 * slab;
+
+  // 3. chunks of whole LORs, reduced in order
+  const int enum_bits = bits_for(n);
+  const int key_bits = enum_bits + bits_for(n_vox);
+  long long first = 0;
+  while (first < n)
+  {
+    long long last = first + 1;
+    while (last < n && off[(size_t)last + 1] - off[(size_t)first] <= max_pairs)
+    {
+      ++last;
+    }
+    const long long m = off[(size_t)last] - off[(size_t)first];
+    if (m > 0)
+    {
+      k_emit<<<blocks_for(last - first, cfg.block), cfg.block, 0, cfg.stream>>>(
+        g, s, t, vals, vals_by_enum ? 1 : 0, (int)first, (int)last, offsets, off[(size_t)first], enum_bits, keys_a,
+        prods_a);
+      size_t tmp = sort_bytes;
+      e = cub::DeviceRadixSort::SortPairs(sort_tmp, tmp, keys_a, keys_b, prods_a, prods_b, (int)m, 0, key_bits,
+                                          cfg.stream);
+      if (e != cudaSuccess)
+      {
+        return e;
+      }
+      k_reduce_runs<<<blocks_for(m, 256), 256, 0, cfg.stream>>>(m, keys_b, prods_b, enum_bits, img);
+      *launches += 2;
+    }
+    first = last;
+  }
+  return cudaGetLastError();
+}
+}  // namespace fir

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <functional>
+
 #include "siddon.cuh"
 
 namespace fir
@@ -40,6 +42,22 @@ void launch_siddon_paths(const Grid& g, long long n, const double* ends, int cap
 void launch_lor_paths(const Grid& g, const Sino& s, const Tables& t, long long n,
                       const long long* bins, int cap, int* coords, double* lengths, int* counts,
                       int* crosses, const LaunchCfg& cfg);
+
+// deterministic.cu
+// ratio[i] = sino / (projection + bias) for enumerated LOR i, or 0
+void launch_ratio(const Grid& g, const Sino& s, const Tables& t, const double* img, const float* sino,
+                  const float* bias, float* ratio, const LaunchCfg& cfg);
+// Device scratch of at least `bytes` for slot 0 (per-LOR counts and
+// offsets) or slot 1 (pairs and sort space); nullptr if unavailable.
+using ScratchFn = std::function<void*(int slot, size_t bytes)>;
+// img += backprojection of vals (per bin, or per enumerated LOR; nullptr =
+// all ones), summed in FIR's serial LOR order with FIR's rounding, in
+// chunks of at most max_pairs_cap (voxel, product) pairs.  Synchronises the
+// stream once, after counting.
+cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables& t, const float* vals,
+                                      bool vals_by_enum, float* img, const ScratchFn& scratch,
+                                      long long max_pairs_cap, long long n_vox, const LaunchCfg& cfg,
+                                      long long* launches);
 
 // image_ops.cu
 constexpr int kMaxHalfTaps = 64;

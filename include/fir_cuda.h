@@ -142,7 +142,11 @@ typedef enum fir_option
   /* 1: bracket every projector-kernel launch (forward, backward,
    * sensitivity, OSEM sub-iteration) with CUDA events on the context's
    * stream; read the accumulated device time with fir_ctx_projector_time. */
-  FIR_OPT_TIMING = 5
+  FIR_OPT_TIMING = 5,
+  /* Deterministic backprojection works on chunks of at most this many
+   * (voxel, contribution) pairs (16 bytes each, twice, plus sort space);
+   * 0 restores the default of 2^28.  Any chunk size gives the same result. */
+  FIR_OPT_DETERMINISTIC_CHUNK = 6
 } fir_option;
 
 enum
