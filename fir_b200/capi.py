@@ -128,6 +128,17 @@ _SIGS = {
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "fir_lor_paths": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.POINTER(VolDesc), C.c_longlong, C.c_void_p,
                                 C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "fir_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_void_p, C.c_int, C.POINTER(ScannerDesc),
+                                   C.POINTER(ProjDesc), C.POINTER(VolDesc), C.POINTER(OsemParamsDesc)]),
+    "fir_batch_destroy": (C.c_int, [C.c_void_p]),
+    "fir_batch_set_data": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "fir_batch_set_image": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "fir_batch_get_image": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "fir_batch_set_launch": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "fir_batch_get_launch": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "fir_batch_tune": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "fir_batch_schedule": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
+    "fir_batch_osem": (C.c_int, [C.c_void_p, C.c_int]),
 }
 
 
@@ -452,3 +463,78 @@ class Context:
                                    bins.ctypes.data, cap, coords.ctypes.data, lengths.ctypes.data,
                                    counts.ctypes.data, crosses.ctypes.data))
         return crosses, counts, coords, lengths
+
+
+class Batch:
+    """A ``fir_batch``: independent OSEM problems run together.
+
+    problems: sequence of (ScannerSpec, ProjSpec, VolSpec, OSEMParams).
+    """
+
+    def __init__(self, ctx: Context, problems):
+        self.ctx = ctx
+        self.problems = list(problems)
+        n = len(self.problems)
+        sc = (ScannerDesc * n)(*[scanner_desc(p[0]) for p in self.problems])
+        pr = (ProjDesc * n)(*[proj_desc(p[1]) for p in self.problems])
+        vo = (VolDesc * n)(*[vol_desc(p[2], 1) for p in self.problems])
+        pa = (OsemParamsDesc * n)(*[osem_desc(p[3]) for p in self.problems])
+        self._h = C.c_void_p()
+        _check(lib().fir_batch_create(C.byref(self._h), ctx.handle, n, sc, pr, vo, pa))
+
+    def close(self) -> None:
+        if self._h:
+            lib().fir_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.problems)
+
+    def set_data(self, p: int, sino, sens, bias=None) -> None:
+        _, proj, vol, prm = self.problems[p]
+        nb = proj_geometry(proj)["n_bins"]
+        _check(lib().fir_batch_set_data(self._h, int(p), _ptr(sino, n=nb),
+                                        _ptr(sens, n=vol.n_voxels * prm.n_subsets), _ptr(bias, n=nb)))
+
+    def _n_voxels(self, p: int):
+        # out-of-range indices are left to the library, which reports them
+        return self.problems[p][2].n_voxels if 0 <= p < len(self.problems) else None
+
+    def set_image(self, p: int, img) -> None:
+        _check(lib().fir_batch_set_image(self._h, int(p), _ptr(img, n=self._n_voxels(p))))
+
+    def get_image(self, p: int, img=None):
+        vol = self.problems[p][2]
+        if img is None:
+            img = np.zeros(vol.shape_zyx, np.float32)
+        _check(lib().fir_batch_get_image(self._h, int(p), _ptr(img, writable=True, n=vol.n_voxels)))
+        return img
+
+    def set_launch(self, block: int, blocks_per_sm: int, grab: int = 1) -> None:
+        _check(lib().fir_batch_set_launch(self._h, int(block), int(blocks_per_sm), int(grab)))
+
+    def launch(self):
+        """(block, blocks_per_sm, grab) of the projector."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().fir_batch_get_launch(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def tune(self) -> float:
+        ms = C.c_double()
+        _check(lib().fir_batch_tune(self._h, C.byref(ms)))
+        return ms.value
+
+    def schedule(self):
+        """(steps, kernel launches) of the whole schedule."""
+        n, k = C.c_int(), C.c_longlong()
+        _check(lib().fir_batch_schedule(self._h, C.byref(n), C.byref(k)))
+        return n.value, k.value
+
+    def osem(self, use_graph: bool = True) -> None:
+        _check(lib().fir_batch_osem(self._h, 1 if use_graph else 0))

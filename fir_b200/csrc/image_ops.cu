@@ -80,17 +80,6 @@ __global__ void k_conv_pass(int nx, int ny, int nz, int axis, Taps taps, const f
   }
 }
 
-__device__ __forceinline__ double radius_of(int x, int y, int nx, int ny, double vx, double vy)
-{
-  // operations.cc:160-185 and :206-212: voxel centre relative to the volume
-  // centre, in double.
-  const double px = __dsub_rn(__dadd_rn(__dmul_rn((double)x, vx), __ddiv_rn(vx, 2.0)),
-                              __ddiv_rn(__dmul_rn((double)nx, vx), 2.0));
-  const double py = __dsub_rn(__dadd_rn(__dmul_rn((double)y, vy), __ddiv_rn(vy, 2.0)),
-                              __ddiv_rn(__dmul_rn((double)ny, vy), 2.0));
-  return __dsqrt_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)));
-}
-
 __global__ void k_conv_restore(int nx, int ny, int nz, double vx, double vy, float cut, float fwhm,
                                const float* __restrict__ copy, float* __restrict__ img)
 {

@@ -81,4 +81,76 @@ void launch_apply_mask(long long n, float* img, const float* mask, const LaunchC
 void launch_hu_to_mu(long long n, float* img, const LaunchCfg& cfg);
 void launch_exponential(long long n, float* sino, const LaunchCfg& cfg);
 void launch_proj_multiply(long long n, float* a, const float* b, const LaunchCfg& cfg);
+
+// Distance of voxel (x, y)'s centre from the volume axis, in FIR's double
+// arithmetic (operations.cc:160-185 and :206-212).
+__device__ __forceinline__ double radius_of(int x, int y, int nx, int ny, double vx, double vy)
+{
+  const double px = __dsub_rn(__dadd_rn(__dmul_rn((double)x, vx), __ddiv_rn(vx, 2.0)),
+                              __ddiv_rn(__dmul_rn((double)nx, vx), 2.0));
+  const double py = __dsub_rn(__dadd_rn(__dmul_rn((double)y, vy), __ddiv_rn(vy, 2.0)),
+                              __ddiv_rn(__dmul_rn((double)ny, vy), 2.0));
+  return __dsqrt_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)));
+}
+
+// batch.cu: many independent OSEM problems per launch.
+// One problem of a batch, resident in device memory.
+struct BatchProblem
+{
+  Grid g;
+  Sino s;  // enumeration for the problem's number of subsets (subset unused)
+  Tables t;
+  const float* sino;
+  const float* bias;  // nullptr: none
+  const float* sens;  // n_subsets frames
+  float* img;
+  double* wide;  // double copy of img for the projector gathers
+  float* bp;
+  float* t1;
+  float* t2;
+  int nvox;
+  int skip_zero;
+  double vx, vy;
+  float cut;   // cut radius (0: none)
+  float fwhm;  // max(fwhm x, fwhm y), for the filter's edge restore
+  Taps tx, ty, tz;
+};
+
+// One problem's share of one batched launch.  Work units are numbered
+// across the items of a launch: bundles of 32 LORs for the projector,
+// blocks of kBatchBlock voxels for the image kernels.
+struct BatchItem
+{
+  int problem;
+  int subset;
+  int filter;  // 1: the sub-iteration filters the image (the filter passes finish it)
+  int unit_begin;
+};
+
+constexpr int kBatchBlock = 256;
+
+struct BatchLaunch
+{
+  int block;          // threads per block of the projector
+  int blocks_per_sm;  // 0: a warp per bundle, no persistence
+  int grab;           // bundles taken per queue access by a persistent warp
+};
+
+// wide = cut(img), bp = 0 (and img = cut(img) when write_img).
+void launch_batch_prepare(const BatchProblem* P, const BatchItem* items, int n_items, int n_units,
+                          bool write_img, cudaStream_t stream);
+// bp += backprojection of measured/estimated for every item's subset.
+// queue: a zeroed counter (persistent mode).
+void launch_batch_project(const BatchProblem* P, const BatchItem* items, int n_items, int n_bundles,
+                          int* queue, const BatchLaunch& L, int n_sms, int* check, cudaStream_t stream);
+// Gated EM update of img; bp <- 0.  Items without filtering also apply the
+// cut and refresh wide.
+void launch_batch_em(const BatchProblem* P, const BatchItem* items, int n_items, int n_units,
+                     cudaStream_t stream);
+// Filter pass along axis (0: img -> t1, 1: t1 -> t2, 2: t2 -> img with the
+// edge restore, the cut and the refresh of wide).
+void launch_batch_filter(const BatchProblem* P, const BatchItem* items, int n_items, int n_units, int axis,
+                         cudaStream_t stream);
+// Resident blocks per SM of the projector at this block size.
+int batch_max_resident(int block);
 }  // namespace fir

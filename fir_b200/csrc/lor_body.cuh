@@ -1,0 +1,73 @@
+// Per-LOR device bodies shared by the single-problem kernels (projector.cu)
+// and the batched persistent kernel (batch.cu).
+#pragma once
+
+#include "internal.h"
+
+namespace fir
+{
+__device__ __forceinline__ void flag(int* check, int bit)
+{
+  if (check != nullptr)
+  {
+    atomicOr(check, bit);
+  }
+}
+
+// The per-LOR body of one OSEM sub-iteration (reconAlgos.cc:119-158 with
+// getLine :11-59) for enumerated index i of `subset`: project the current
+// image along the LOR, add the bias, and if the estimate exceeds 1e-5
+// backproject measured/estimated along the same path.  The path is
+// traversed twice from the same saved setup, so both traversals visit
+// identical voxels with identical lengths.  Every lane of the warp must call
+// this (lanes with i >= n_enum are idle), since it re-converges the warp
+// between the traversals.
+__device__ __forceinline__ void osem_lor(const Grid& g, const Sino& s, int subset, const Tables& t,
+                                         const double* __restrict__ img, const float* __restrict__ sino,
+                                         const float* __restrict__ bias, float* bp, bool skip_zero, int i,
+                                         int* check)
+{
+  const bool valid = i < s.n_enum;
+  Lor l{};
+  Walk w{};
+  bool go = false;
+  float y = 0.0f;
+  if (valid)
+  {
+    l = decode_bin(s, i, subset);
+    y = __ldg(sino + l.bin);
+    // With y == 0 the ratio is exactly 0 whatever the estimate, so the bin
+    // contributes nothing: skipping it is exact.
+    if (!(skip_zero && y == 0.0f))
+    {
+      double e[6];
+      lor_ends(s, t, l, e);
+      go = siddon_setup(g, e, w);
+    }
+  }
+  float line = 0.0f;
+  bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
+    if (inside)
+    {
+      line = accumulate(line, len, __ldg(img + c));
+    }
+  });
+  __syncwarp();
+  if (valid && bias != nullptr)
+  {
+    line = __fadd_rn(line, __ldg(bias + l.bin));
+  }
+  const bool back = go && ok && (double)line > kEps;
+  const double ratio = back ? (double)__fdiv_rn(y, line) : 0.0;
+  ok = siddon_walk(g, w, back, [&](bool inside, int c, double len) {
+         if (inside)
+         {
+           atomicAdd(bp + c, __double2float_rn(dmul(len, ratio)));
+         }
+       }) && ok;
+  if (!ok)
+  {
+    flag(check, kCheckWalkGuard);
+  }
+}
+}  // namespace fir

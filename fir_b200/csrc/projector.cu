@@ -12,20 +12,12 @@
 // recomputed on the fly (no LOR cache, no stored path).  The image is
 // gathered from a double-precision copy (exact widening of the float image,
 // made once per call), which stays resident in the 126 MB L2.
-#include "internal.h"
+#include "lor_body.cuh"
 
 namespace fir
 {
 namespace
 {
-__device__ __forceinline__ void flag(int* check, int bit)
-{
-  if (check != nullptr)
-  {
-    atomicOr(check, bit);
-  }
-}
-
 // projections::forward (projections.cc:15-92) with
 // VolData::computeLineIntegral (VolData.cc:357-371); optional epilogue
 // ProjData::exponential (ProjData.cc:514-539).
@@ -105,11 +97,8 @@ __global__ void __launch_bounds__(256) k_backward(Grid g, Sino s, Tables t,
   }
 }
 
-// The per-LOR body of one OSEM sub-iteration (reconAlgos.cc:119-158 with
-// getLine :11-59): project the current image along the LOR, add the bias,
-// and if the estimate exceeds 1e-5 backproject measured/estimated along the
-// same path.  The path is traversed twice from the same saved setup, so both
-// traversals visit identical voxels with identical lengths.
+// One OSEM sub-iteration over the subset of s: one thread per enumerated
+// LOR (reconAlgos.cc:119-158).
 __global__ void __launch_bounds__(256) k_osem_subset(Grid g, Sino s, Tables t,
                                                      const double* __restrict__ img,
                                                      const float* __restrict__ sino,
@@ -117,48 +106,7 @@ __global__ void __launch_bounds__(256) k_osem_subset(Grid g, Sino s, Tables t,
                                                      int skip_zero, int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = i < s.n_enum;
-  Lor l{};
-  Walk w{};
-  bool go = false;
-  float y = 0.0f;
-  if (valid)
-  {
-    l = decode_bin(s, i);
-    y = __ldg(sino + l.bin);
-    // With y == 0 the ratio is exactly 0 whatever the estimate, so the bin
-    // contributes nothing: skipping it is exact.
-    if (!(skip_zero && y == 0.0f))
-    {
-      double e[6];
-      lor_ends(s, t, l, e);
-      go = siddon_setup(g, e, w);
-    }
-  }
-  float line = 0.0f;
-  bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
-    if (inside)
-    {
-      line = accumulate(line, len, __ldg(img + c));
-    }
-  });
-  __syncwarp();
-  if (valid && bias != nullptr)
-  {
-    line = __fadd_rn(line, __ldg(bias + l.bin));
-  }
-  const bool back = go && ok && (double)line > kEps;
-  const double ratio = back ? (double)__fdiv_rn(y, line) : 0.0;
-  ok = siddon_walk(g, w, back, [&](bool inside, int c, double len) {
-         if (inside)
-         {
-           atomicAdd(bp + c, __double2float_rn(dmul(len, ratio)));
-         }
-       }) && ok;
-  if (!ok)
-  {
-    flag(check, kCheckWalkGuard);
-  }
+  osem_lor(g, s, s.subset, t, img, sino, bias, bp, skip_zero != 0, i, check);
 }
 
 // Path dump of one segment into row i of coords / lengths.

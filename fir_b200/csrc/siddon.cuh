@@ -61,8 +61,9 @@ __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a,
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
 
-// Enumerated index -> bin coordinates.
-__device__ __forceinline__ Lor decode_bin(const Sino& s, int i)
+// Enumerated index -> bin coordinates, for subset `subset` of s.n_subsets
+// (the enumeration bases depend only on the number of subsets).
+__device__ __forceinline__ Lor decode_bin(const Sino& s, int i, int subset)
 {
   int lo = 0, hi = s.n_segments;
   while (hi - lo > 1)
@@ -80,13 +81,15 @@ __device__ __forceinline__ Lor decode_bin(const Sino& s, int i)
   const int rem = r - sv * bpv;
   const int ax = rem / s.n_tang;
   Lor l;
-  l.view = sv * s.n_subsets + s.subset;
+  l.view = sv * s.n_subsets + subset;
   l.seg = lo - s.seg_offset;
   l.axial = ax;
   l.tang = rem - ax * s.n_tang - s.tang_offset;
   l.bin = s.seg_base[lo] + l.view * bpv + rem;
   return l;
 }
+
+__device__ __forceinline__ Lor decode_bin(const Sino& s, int i) { return decode_bin(s, i, s.subset); }
 
 // ProjData::getCrystalAxialCoord (ProjData.cc:198-299): slice indices.
 __device__ __forceinline__ void crystal_axial(const Sino& s, int seg, int axial, int& a1, int& a2)

@@ -136,13 +136,15 @@ def batch_problems(n: int = 64, seed: int = 3) -> List[Workload]:
     out = []
     for i in range(n):
         n_rings = int(rng.integers(4, 25))
-        n_cpr = 4 * int(rng.integers(24, 97))
+        # crystals: a multiple of 4 whose number of views has a divisor in [4, 12]
+        divisors = []
+        while not divisors:
+            n_cpr = 4 * int(rng.integers(24, 97))
+            divisors = [d for d in range(4, 13) if (n_cpr // 2) % d == 0]
         radius = float(rng.uniform(150.0, 400.0))
         vox = float(rng.choice([2.0, 3.0, 4.0]))
         nxy = int(rng.integers(32, 129))
         nz = int(rng.integers(8, 49))
-        n_views = n_cpr // 2
-        divisors = [d for d in range(4, 13) if n_views % d == 0] or [2]
         n_sub = int(rng.choice(divisors))
         half_width = nxy * vox / 2.0
         fov = min(0.9 * half_width, 0.7 * radius)
@@ -226,3 +228,34 @@ def poisson_counts(expected: np.ndarray, total: float, seed: int) -> np.ndarray:
     s = float(expected.sum(dtype=np.float64))
     lam = expected.astype(np.float64) * (total / s if s > 0 else 0.0)
     return np.random.default_rng(seed).poisson(lam).astype(np.float32)
+
+
+def measured_on_gpu(ctx, w: Workload, device, attenuation: bool = True):
+    """Measured data of ``w`` made with the GPU projector of ``ctx`` (scanner
+    and geometry already set): the phantom is forward-projected, divided by
+    the attenuation factors exp(A mu) when ``attenuation``, scaled to
+    ``w.counts``, Poisson-sampled with ``w.seed`` and precorrected by the
+    factors again (OSEM.cc:294-337).  Returns (sinogram, sensitivity with
+    ``w.osem.n_subsets`` frames) as device tensors."""
+    import torch
+
+    nb = w.n_lors
+    x_true = torch.from_numpy(activity(w)).to(device)
+    ax = torch.empty(nb, device=device)
+    ctx.forward(w.vol, x_true, w.proj, ax)
+    acf = None
+    if attenuation:
+        mu = torch.from_numpy(hounsfield(w)).to(device)
+        ctx.hu_to_mu(w.vol, mu)
+        acf = torch.empty(nb, device=device)
+        ctx.forward_exp(w.vol, mu, w.proj, acf)
+        ax = ax / acf
+    ax *= w.counts / float(ax.sum(dtype=torch.float64))
+    gen = torch.Generator(device=device).manual_seed(w.seed)
+    y = torch.poisson(ax, generator=gen)
+    if acf is not None:
+        ctx.proj_multiply(w.proj, y, acf)
+    nsub = w.osem.n_subsets
+    sens = torch.empty((nsub,) + tuple(w.vol.shape_zyx), device=device)
+    ctx.sensitivity(w.proj, w.vol, sens, nsub)
+    return y, sens

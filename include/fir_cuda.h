@@ -272,6 +272,56 @@ fir_status fir_osem(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, 
                     const fir_vol_desc* vol, float* img, const float* sens,
                     const fir_osem_params* params, fir_osem_save_fn save, void* user);
 
+/* ---- batched OSEM: many independent reconstructions at once ----
+ *
+ * No counterpart in FIR, which reconstructs one problem per process.  A
+ * batch holds n problems, each with its own scanner, sinogram geometry,
+ * volume (one frame) and OSEM parameters, of any sizes.  fir_batch_osem runs
+ * reconAlgos::OSEM (reconAlgos.cc:63-201) on all of them together: step t
+ * performs sub-iteration t of every problem that has one, with one
+ * persistent launch for the projection/backprojection of all those
+ * problems' LORs and one launch per image operation for all their images.
+ * The schedule can be captured once in a CUDA graph and replayed.  Each
+ * problem's result is that of fir_osem on it, up to the order of the float
+ * atomic additions of the backprojection.
+ *
+ * The batch owns device copies of all its data (sinograms, sensitivities,
+ * optional biases, images, scratch) and runs on a stream of its own, ordered
+ * after and before the context's stream: work queued on the context's
+ * stream before fir_batch_osem runs before it, and work queued after it
+ * runs after it.  The context's geometry and skip-zero options at creation
+ * apply. */
+typedef struct fir_batch fir_batch;
+
+fir_status fir_batch_create(fir_batch** batch, fir_ctx* ctx, int n_problems, const fir_scanner_desc* scanners,
+                            const fir_proj_desc* projs, const fir_vol_desc* vols, const fir_osem_params* params);
+fir_status fir_batch_destroy(fir_batch* batch);
+/* Copies problem p's measured sinogram, its sensitivity (n_subsets frames)
+ * and its bias sinogram (NULL: none) into the batch; host or device
+ * pointers; returns when the copies are done. */
+fir_status fir_batch_set_data(fir_batch* batch, int p, const float* sino, const float* sens, const float* bias);
+fir_status fir_batch_set_image(fir_batch* batch, int p, const float* img);
+/* Waits for the batch's work and reports device-side check failures. */
+fir_status fir_batch_get_image(fir_batch* batch, int p, float* img);
+/* Launch shape of the projector: threads per block (32..256, a multiple of
+ * 32), resident blocks per SM (0: one warp per bundle of 32 LORs, no
+ * persistence; otherwise a persistent grid of that many blocks per SM,
+ * capped at what fits), and bundles taken per queue access (1..64). */
+fir_status fir_batch_set_launch(fir_batch* batch, int block, int blocks_per_sm, int grab);
+fir_status fir_batch_get_launch(const fir_batch* batch, int* block, int* blocks_per_sm, int* grab);
+/* Autotuner: times the projector of step 0 (all problems' first subsets) for
+ * each candidate launch shape and keeps the fastest; *best_ms (may be NULL)
+ * receives its time.  It uses the current images without changing them. */
+fir_status fir_batch_tune(fir_batch* batch, double* best_ms);
+/* Number of steps (the largest number of sub-iterations of any problem) and
+ * number of kernel launches of the whole schedule. */
+fir_status fir_batch_schedule(const fir_batch* batch, int* n_steps, long long* n_launches);
+/* Runs every problem's OSEM (initial cut, then all sub-iterations) in place
+ * on the batch's images; asynchronous.  use_graph != 0 captures the schedule
+ * in a CUDA graph on first use (and after a launch-shape change) and
+ * replays it; 0 launches the kernels one by one. */
+fir_status fir_batch_osem(fir_batch* batch, int use_graph);
+
 /* ---- image and sinogram operations ---- */
 fir_status fir_em_update(fir_ctx* ctx, const fir_vol_desc* vol, float* img, float* bp,
                          const float* sens_frame);
