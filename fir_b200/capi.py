@@ -29,6 +29,8 @@ FIR_GEOMETRY_REFERENCE = 0
 FIR_GEOMETRY_EXACT = 1
 FIR_BACKPROJ_ATOMIC = 0
 FIR_BACKPROJ_DETERMINISTIC = 1
+FIR_F32 = 0
+FIR_F64 = 1
 
 
 class FirError(RuntimeError):
@@ -128,6 +130,10 @@ _SIGS = {
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "fir_lor_paths": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.POINTER(VolDesc), C.c_longlong, C.c_void_p,
                                 C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "fir_forward_frames": (C.c_int, [C.c_void_p, C.POINTER(VolDesc), C.c_void_p, C.POINTER(ProjDesc), C.c_void_p,
+                                     C.c_int]),
+    "fir_backward_frames": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.c_void_p, C.POINTER(VolDesc), C.c_void_p,
+                                      C.c_int]),
     "fir_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_void_p, C.c_int, C.POINTER(ScannerDesc),
                                    C.POINTER(ProjDesc), C.POINTER(VolDesc), C.POINTER(OsemParamsDesc)]),
     "fir_batch_destroy": (C.c_int, [C.c_void_p]),
@@ -256,6 +262,17 @@ def _ptr(x, dtype=np.float32, writable=False, n: Optional[int] = None):
     if n is not None and x.size < n:
         raise ValueError(f"buffer holds {x.size} elements, {n} required")
     return x.ctypes.data
+
+
+def _dtype_of(x):
+    try:
+        import torch
+
+        if isinstance(x, torch.Tensor):
+            return np.float64 if x.dtype == torch.float64 else np.float32
+    except ImportError:
+        pass
+    return np.float64 if np.asarray(x).dtype == np.float64 else np.float32
 
 
 class Context:
@@ -438,6 +455,28 @@ class Context:
                                        _ptr(b, n=nb)))
 
     # -- path dumps
+    def _frames_args(self, vol: VolSpec, img, proj: ProjSpec, sino):
+        n_frames = img.shape[0] if img.ndim == 4 else 1
+        dt = np.float64 if _dtype_of(img) == np.float64 else np.float32
+        if _dtype_of(sino) != dt:
+            raise TypeError("image and sinogram must have the same dtype")
+        nb = proj_geometry(proj)["n_bins"]
+        return (vol_desc(vol, n_frames), _ptr(img, dt, n=vol.n_voxels * n_frames), _ptr(sino, dt, n=nb * n_frames),
+                FIR_F64 if dt == np.float64 else FIR_F32)
+
+    def forward_frames(self, vol: VolSpec, img, proj: ProjSpec, sino) -> None:
+        """sino[f] = projection of img[f] for every frame ([F, nz, ny, nx] ->
+        [F, n_bins]); float32 (FIR's arithmetic) or float64."""
+        self._prep(img, sino)
+        vd, pi, ps, dt = self._frames_args(vol, img, proj, sino)
+        _check(lib().fir_forward_frames(self._h, C.byref(vd), pi, C.byref(proj_desc(proj)), ps, dt))
+
+    def backward_frames(self, proj: ProjSpec, sino, vol: VolSpec, img) -> None:
+        """img[f] = backprojection of sino[f] (the adjoint of forward_frames)."""
+        self._prep(img, sino)
+        vd, pi, ps, dt = self._frames_args(vol, img, proj, sino)
+        _check(lib().fir_backward_frames(self._h, C.byref(proj_desc(proj)), ps, C.byref(vd), pi, dt))
+
     def siddon_paths(self, vol: VolSpec, ends, cap: Optional[int] = None):
         ends = np.ascontiguousarray(ends, np.float64).reshape(-1, 6)
         n = ends.shape[0]

@@ -482,7 +482,7 @@ struct fir_ctx
   DevBuf check;     // device check word
   int* check_host = nullptr;  // pinned mirror
 
-  DevBuf bp, conv1, conv2, conv_copy, mu, wide, det, det_pairs, ratio;
+  DevBuf bp, conv1, conv2, conv_copy, mu, wide, det, det_pairs, ratio, frames_il, frames_acc;
   std::vector<DevBuf> staging;
 
   // projector-kernel timing (FIR_OPT_TIMING)
@@ -1049,7 +1049,7 @@ fir_status fir_ctx_destroy(fir_ctx* c)
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     for (DevBuf* b : {&c->xy, &c->z, &c->check, &c->bp, &c->conv1, &c->conv2, &c->conv_copy, &c->mu, &c->wide,
-                      &c->det, &c->det_pairs, &c->ratio})
+                      &c->det, &c->det_pairs, &c->ratio, &c->frames_il, &c->frames_acc})
     {
       b->release();
     }
@@ -1266,6 +1266,86 @@ fir_status fir_backward(fir_ctx* ctx, const fir_proj_desc* proj, const float* si
       timed_launch(c, [&] {
         launch_backward(g, ss, t, dsino, dimg + (size_t)s * v.nvox, c.skip_zero != 0, cfg_of(c));
       });
+    }
+    finish(c, st);
+  });
+}
+
+static bool check_dtype(fir_dtype d)
+{
+  if (d != FIR_F32 && d != FIR_F64)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "unknown data type ", (int)d);
+  }
+  return d == FIR_F64;
+}
+
+fir_status fir_forward_frames(fir_ctx* ctx, const fir_vol_desc* vol, const void* img, const fir_proj_desc* proj,
+                              void* sino, fir_dtype dtype)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const VolInfo v = check_vol(vol);
+    const ProjInfo p = check_proj(proj);
+    const bool f64 = check_dtype(dtype);
+    const Tables t = tables_of(c, p);
+    const Grid g = grid_of(c, v);
+    if (img == nullptr || sino == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "image and sinogram must not be NULL");
+    }
+    const long long es = f64 ? 8 : 4;
+    const int nfr = v.d.n_frames;
+    Stager st(c);
+    const char* dimg = st.in(static_cast<const char*>(img), v.nvox * nfr * es);
+    char* dsino = st.out(static_cast<char*>(sino), p.g.n_bins * nfr * es);
+    const Sino s = sino_of(p, 1, 0);
+    for (int f0 = 0; f0 < nfr; f0 += kMaxFramesPerPass)
+    {
+      const int nf = std::min(kMaxFramesPerPass, nfr - f0);
+      auto* il = static_cast<double*>(c.frames_il.ensure((size_t)v.nvox * frames_stride(nf) * sizeof(double)));
+      launch_interleave(v.nvox, nf, dimg + (size_t)f0 * v.nvox * es, f64, il, cfg_of(c));
+      after_launch(c);
+      timed_launch(c, [&] {
+        launch_forward_frames(g, s, t, il, nf, p.g.n_bins, dsino + (size_t)f0 * p.g.n_bins * es, f64, cfg_of(c));
+      });
+    }
+    finish(c, st);
+  });
+}
+
+fir_status fir_backward_frames(fir_ctx* ctx, const fir_proj_desc* proj, const void* sino, const fir_vol_desc* vol,
+                               void* img, fir_dtype dtype)
+{
+  return guarded([&] {
+    fir_ctx& c = check_ctx(ctx);
+    const ProjInfo p = check_proj(proj);
+    const VolInfo v = check_vol(vol);
+    const bool f64 = check_dtype(dtype);
+    const Tables t = tables_of(c, p);
+    const Grid g = grid_of(c, v);
+    if (img == nullptr || sino == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "image and sinogram must not be NULL");
+    }
+    const long long es = f64 ? 8 : 4;
+    const int nfr = v.d.n_frames;
+    Stager st(c);
+    const char* dsino = st.in(static_cast<const char*>(sino), p.g.n_bins * nfr * es);
+    char* dimg = st.out(static_cast<char*>(img), v.nvox * nfr * es);
+    const Sino s = sino_of(p, 1, 0);
+    for (int f0 = 0; f0 < nfr; f0 += kMaxFramesPerPass)
+    {
+      const int nf = std::min(kMaxFramesPerPass, nfr - f0);
+      const size_t acc_bytes = (size_t)v.nvox * frames_stride(nf) * es;
+      void* acc = c.frames_acc.ensure(acc_bytes);
+      cuda_ok(cudaMemsetAsync(acc, 0, acc_bytes, c.stream), "cudaMemsetAsync");
+      timed_launch(c, [&] {
+        launch_backward_frames(g, s, t, dsino + (size_t)f0 * p.g.n_bins * es, nf, p.g.n_bins, acc, f64,
+                               c.skip_zero != 0, cfg_of(c));
+      });
+      launch_deinterleave(v.nvox, nf, acc, f64, dimg + (size_t)f0 * v.nvox * es, cfg_of(c));
+      after_launch(c);
     }
     finish(c, st);
   });

@@ -1,0 +1,259 @@
+// Multi-frame projection: several images projected (or sinograms
+// backprojected) with one traversal per LOR.
+//
+// FIR projects a multi-frame volume frame by frame (ForwardProj.cc:79-100),
+// tracing every path once per frame.  Here a thread traces its LOR once and
+// gathers (or scatters) all frames of a group of up to 8 at every step.  The
+// frames of a group are interleaved in device scratch, voxel-major
+// ([voxel][frame], stride FMAX), so the frames of one voxel share one or two
+// 32-byte sectors: the traversal, which dominates the cost, is paid once per
+// group instead of once per frame.
+//
+// Two arithmetics:
+// * FIR_F32: per frame exactly fir_forward / fir_backward (float running sum
+//   widened and rounded per step; float atomics of float(len * value));
+// * FIR_F64: double data, double running sums and double atomics, for
+//   gradient checks that need more than float resolution.
+#include "lor_body.cuh"
+
+namespace fir
+{
+namespace
+{
+template<int FMAX, bool F64>
+__global__ void __launch_bounds__(256) k_forward_frames(Grid g, Sino s, Tables t, const double* __restrict__ il,
+                                                        int nf, long long n_bins, void* out, int* check)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = i < s.n_enum;
+  Lor l{};
+  Walk w{};
+  bool go = false;
+  if (valid)
+  {
+    l = decode_bin(s, i);
+    double e[6];
+    lor_ends(s, t, l, e);
+    go = siddon_setup(g, e, w);
+  }
+  float lf[FMAX];
+  double ld[FMAX];
+#pragma unroll
+  for (int f = 0; f < FMAX; ++f)
+  {
+    lf[f] = 0.0f;
+    ld[f] = 0.0;
+  }
+  const bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
+    if (inside)
+    {
+      const double* v = il + (size_t)c * FMAX;
+#pragma unroll
+      for (int f = 0; f < FMAX; ++f)
+      {
+        if (f < nf)
+        {
+          const double x = __ldg(v + f);
+          if (F64)
+            ld[f] = dadd(ld[f], dmul(len, x));
+          else
+            lf[f] = accumulate(lf[f], len, x);
+        }
+      }
+    }
+  });
+  if (!ok)
+  {
+    flag(check, kCheckWalkGuard);
+  }
+  if (valid)
+  {
+#pragma unroll
+    for (int f = 0; f < FMAX; ++f)
+    {
+      if (f < nf)
+      {
+        if (F64)
+          static_cast<double*>(out)[f * n_bins + l.bin] = ld[f];
+        else
+          static_cast<float*>(out)[f * n_bins + l.bin] = lf[f];
+      }
+    }
+  }
+}
+
+template<int FMAX, bool F64>
+__global__ void __launch_bounds__(256) k_backward_frames(Grid g, Sino s, Tables t, const void* __restrict__ sino,
+                                                         int nf, long long n_bins, void* acc, int skip_zero,
+                                                         int* check)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  Walk w{};
+  bool go = false;
+  double v[FMAX];
+#pragma unroll
+  for (int f = 0; f < FMAX; ++f)
+  {
+    v[f] = 0.0;
+  }
+  if (i < s.n_enum)
+  {
+    const Lor l = decode_bin(s, i);
+    bool any = false;
+#pragma unroll
+    for (int f = 0; f < FMAX; ++f)
+    {
+      if (f < nf)
+      {
+        v[f] = F64 ? __ldg(static_cast<const double*>(sino) + f * n_bins + l.bin)
+                   : (double)__ldg(static_cast<const float*>(sino) + f * n_bins + l.bin);
+        any = any || v[f] != 0.0;
+      }
+    }
+    // with every value 0 every contribution is exactly 0
+    if (!(skip_zero && !any))
+    {
+      double e[6];
+      lor_ends(s, t, l, e);
+      go = siddon_setup(g, e, w);
+    }
+  }
+  const bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
+    if (inside)
+    {
+#pragma unroll
+      for (int f = 0; f < FMAX; ++f)
+      {
+        if (f < nf)
+        {
+          if (F64)
+            atomicAdd(static_cast<double*>(acc) + (size_t)c * FMAX + f, dmul(len, v[f]));
+          else
+            atomicAdd(static_cast<float*>(acc) + (size_t)c * FMAX + f, __double2float_rn(dmul(len, v[f])));
+        }
+      }
+    }
+  });
+  if (!ok)
+  {
+    flag(check, kCheckWalkGuard);
+  }
+}
+
+// il[j * fmax + f] = frame f of img at voxel j (widened), 0 for f >= nf.
+template<typename T>
+__global__ void k_interleave(long long nvox, int nf, int fmax, const T* __restrict__ img, double* __restrict__ il)
+{
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= nvox * fmax)
+  {
+    return;
+  }
+  const long long j = k / fmax;
+  const int f = (int)(k - j * fmax);
+  il[k] = f < nf ? (double)img[(size_t)f * nvox + j] : 0.0;
+}
+
+// img[f][j] = acc[j * fmax + f] for f < nf.
+template<typename T>
+__global__ void k_deinterleave(long long nvox, int nf, int fmax, const T* __restrict__ acc, T* __restrict__ img)
+{
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= nvox * nf)
+  {
+    return;
+  }
+  const int f = (int)(k / nvox);
+  const long long j = k - (long long)f * nvox;
+  img[k] = acc[j * fmax + f];
+}
+
+unsigned blocks_for(long long n, int block)
+{
+  return (unsigned)((n + block - 1) / block);
+}
+
+template<int FMAX>
+void fwd(const Grid& g, const Sino& s, const Tables& t, const double* il, int nf, long long n_bins, void* out,
+         bool f64, const LaunchCfg& cfg)
+{
+  const unsigned nb = blocks_for(s.n_enum, cfg.block);
+  if (f64)
+    k_forward_frames<FMAX, true><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, il, nf, n_bins, out, cfg.check);
+  else
+    k_forward_frames<FMAX, false><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, il, nf, n_bins, out, cfg.check);
+}
+
+template<int FMAX>
+void bwd(const Grid& g, const Sino& s, const Tables& t, const void* sino, int nf, long long n_bins, void* acc,
+         bool f64, bool skip_zero, const LaunchCfg& cfg)
+{
+  const unsigned nb = blocks_for(s.n_enum, cfg.block);
+  if (f64)
+    k_backward_frames<FMAX, true><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, sino, nf, n_bins, acc,
+                                                                     skip_zero ? 1 : 0, cfg.check);
+  else
+    k_backward_frames<FMAX, false><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, sino, nf, n_bins, acc,
+                                                                      skip_zero ? 1 : 0, cfg.check);
+}
+}  // namespace
+
+int frames_stride(int nf)
+{
+  return nf <= 1 ? 1 : (nf <= 2 ? 2 : (nf <= 4 ? 4 : kMaxFramesPerPass));
+}
+
+void launch_interleave(long long nvox, int nf, const void* img, bool f64, double* il, const LaunchCfg& cfg)
+{
+  const int fmax = frames_stride(nf);
+  const unsigned nb = blocks_for(nvox * fmax, 256);
+  if (f64)
+    k_interleave<double><<<nb, 256, 0, cfg.stream>>>(nvox, nf, fmax, static_cast<const double*>(img), il);
+  else
+    k_interleave<float><<<nb, 256, 0, cfg.stream>>>(nvox, nf, fmax, static_cast<const float*>(img), il);
+}
+
+void launch_deinterleave(long long nvox, int nf, const void* acc, bool f64, void* img, const LaunchCfg& cfg)
+{
+  const int fmax = frames_stride(nf);
+  const unsigned nb = blocks_for(nvox * nf, 256);
+  if (f64)
+    k_deinterleave<double><<<nb, 256, 0, cfg.stream>>>(nvox, nf, fmax, static_cast<const double*>(acc),
+                                                       static_cast<double*>(img));
+  else
+    k_deinterleave<float><<<nb, 256, 0, cfg.stream>>>(nvox, nf, fmax, static_cast<const float*>(acc),
+                                                      static_cast<float*>(img));
+}
+
+void launch_forward_frames(const Grid& g, const Sino& s, const Tables& t, const double* il, int nf, long long n_bins,
+                           void* out, bool f64, const LaunchCfg& cfg)
+{
+  if (s.n_enum == 0 || nf <= 0)
+  {
+    return;
+  }
+  switch (frames_stride(nf))
+  {
+    case 1: fwd<1>(g, s, t, il, nf, n_bins, out, f64, cfg); break;
+    case 2: fwd<2>(g, s, t, il, nf, n_bins, out, f64, cfg); break;
+    case 4: fwd<4>(g, s, t, il, nf, n_bins, out, f64, cfg); break;
+    default: fwd<kMaxFramesPerPass>(g, s, t, il, nf, n_bins, out, f64, cfg); break;
+  }
+}
+
+void launch_backward_frames(const Grid& g, const Sino& s, const Tables& t, const void* sino, int nf,
+                            long long n_bins, void* acc, bool f64, bool skip_zero, const LaunchCfg& cfg)
+{
+  if (s.n_enum == 0 || nf <= 0)
+  {
+    return;
+  }
+  switch (frames_stride(nf))
+  {
+    case 1: bwd<1>(g, s, t, sino, nf, n_bins, acc, f64, skip_zero, cfg); break;
+    case 2: bwd<2>(g, s, t, sino, nf, n_bins, acc, f64, skip_zero, cfg); break;
+    case 4: bwd<4>(g, s, t, sino, nf, n_bins, acc, f64, skip_zero, cfg); break;
+    default: bwd<kMaxFramesPerPass>(g, s, t, sino, nf, n_bins, acc, f64, skip_zero, cfg); break;
+  }
+}
+}  // namespace fir

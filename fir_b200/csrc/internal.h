@@ -153,4 +153,19 @@ void launch_batch_filter(const BatchProblem* P, const BatchItem* items, int n_it
                          cudaStream_t stream);
 // Resident blocks per SM of the projector at this block size.
 int batch_max_resident(int block);
+
+// frames.cu: several frames per traversal (groups of up to kMaxFramesPerPass).
+constexpr int kMaxFramesPerPass = 8;
+// Interleave stride of a group of nf frames: 1, 2, 4 or 8.
+int frames_stride(int nf);
+// il[j * stride + f] = (double) frame f of img (float or double, frame-major).
+void launch_interleave(long long nvox, int nf, const void* img, bool f64, double* il, const LaunchCfg& cfg);
+// img[f][j] = acc[j * stride + f] (float or double).
+void launch_deinterleave(long long nvox, int nf, const void* acc, bool f64, void* img, const LaunchCfg& cfg);
+// out[f * n_bins + bin] = projection of frame f (float or double sinograms).
+void launch_forward_frames(const Grid& g, const Sino& s, const Tables& t, const double* il, int nf, long long n_bins,
+                           void* out, bool f64, const LaunchCfg& cfg);
+// acc[c * stride + f] += backprojection of sino[f * n_bins + ...].
+void launch_backward_frames(const Grid& g, const Sino& s, const Tables& t, const void* sino, int nf,
+                            long long n_bins, void* acc, bool f64, bool skip_zero, const LaunchCfg& cfg);
 }  // namespace fir

@@ -17,6 +17,8 @@ benchmark configurations:
                   within 160 mm; 320x320x128 image at 1.5 mm (exact geometry);
                   40 ellipsoids + 20 hot spheres; 2e9 counts; 28 subsets x 1.
 * ``batched``  -- 64 small problems of uneven sizes (``batch_problems``).
+* ``autograd`` -- the clinical scanner with 8 ellipsoid phantoms on a
+                  128x128x48 image at 3 mm (``autograd_batch``).
 
 The phantom arrays are float32 ``[nz, ny, nx]``.  Measured data are made by
 the caller's forward projector: ``expected = scale * A x / ACF`` with the
@@ -111,6 +113,25 @@ def large(seed: int = 5) -> Workload:
         kind="body",
         extra={"body": (155.0, 115.0), "n_ellipsoids": 40, "n_spheres": 20},
     )
+
+
+def autograd_batch(n: int = 8, seed: int = 11) -> List[Workload]:
+    """The differentiable-projector workload: the clinical scanner and
+    field of view, ``n`` seeded ellipsoid phantoms (elliptical water body with
+    10 ellipsoids) on a 128x128x48 image at 3 mm, 5e8 counts each."""
+    base = clinical()
+    rng = np.random.default_rng(seed)
+    return [Workload(
+        name=f"autograd{i}",
+        scanner=base.scanner,
+        proj=base.proj,
+        vol=VolSpec.centred((128, 128, 48), (3.0, 3.0, 3.0)),
+        osem=base.osem,
+        counts=5e8,
+        seed=int(rng.integers(1 << 30)),
+        kind="body",
+        extra={"body": (150.0, 110.0), "n_ellipsoids": 10},
+    ) for i in range(n)]
 
 
 def tiny(seed: int = 0) -> Workload:

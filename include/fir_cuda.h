@@ -272,6 +272,30 @@ fir_status fir_osem(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, 
                     const fir_vol_desc* vol, float* img, const float* sens,
                     const fir_osem_params* params, fir_osem_save_fn save, void* user);
 
+/* ---- multi-frame projection ----
+ *
+ * Element type of the multi-frame projectors' data. */
+typedef enum fir_dtype
+{
+  FIR_F32 = 0, /* float data; per frame FIR's arithmetic */
+  FIR_F64 = 1  /* double data, double sums and double atomics */
+} fir_dtype;
+
+/* Forward projection of the n_frames frames of vol (frame-major images) into
+ * n_frames sinograms (frame-major), tracing each LOR once for a group of up to
+ * 8 frames.  FIR_F32: frame f's sinogram equals fir_forward of frame f.
+ * Counterpart: the frame loop of ForwardProj.cc:79-100 around
+ * projections::forward (projections.cc:15-92). */
+fir_status fir_forward_frames(fir_ctx* ctx, const fir_vol_desc* vol, const void* img, const fir_proj_desc* proj,
+                              void* sino, fir_dtype dtype);
+/* Backprojection of n_frames sinograms into the n_frames frames of vol
+ * (overwritten): the adjoint of fir_forward_frames.  FIR_F32: frame f equals
+ * fir_backward of sinogram f with one subset, up to the order of the float
+ * atomic additions.  Counterpart: projections::backward (projections.cc:94-184)
+ * once per frame. */
+fir_status fir_backward_frames(fir_ctx* ctx, const fir_proj_desc* proj, const void* sino, const fir_vol_desc* vol,
+                               void* img, fir_dtype dtype);
+
 /* ---- batched OSEM: many independent reconstructions at once ----
  *
  * No counterpart in FIR, which reconstructs one problem per process.  A
