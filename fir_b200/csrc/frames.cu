@@ -3,7 +3,7 @@
 //
 // FIR projects a multi-frame volume frame by frame (ForwardProj.cc:79-100),
 // tracing every path once per frame.  Here a thread traces its LOR once and
-// gathers (or scatters) all frames of a group of up to 8 at every step.  The
+// gathers (or scatters) all frames of a group of up to 4 at every step.  The
 // frames of a group are interleaved in device scratch, voxel-major
 // ([voxel][frame], stride FMAX), so the frames of one voxel share one or two
 // 32-byte sectors: the traversal, which dominates the cost, is paid once per
@@ -20,6 +20,18 @@ namespace fir
 {
 namespace
 {
+// Vector float reductions in global memory (sm_90 and later); the address
+// is 16-byte (v4) or 8-byte (v2) aligned.
+__device__ __forceinline__ void red_add_v4(float* p, float a, float b, float c, float d)
+{
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
+}
+
+__device__ __forceinline__ void red_add_v2(float* p, float a, float b)
+{
+  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b) : "memory");
+}
+
 template<int FMAX, bool F64>
 __global__ void __launch_bounds__(256) k_forward_frames(Grid g, Sino s, Tables t, const double* __restrict__ il,
                                                         int nf, long long n_bins, void* out, int* check)
@@ -47,17 +59,32 @@ __global__ void __launch_bounds__(256) k_forward_frames(Grid g, Sino s, Tables t
   const bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
     if (inside)
     {
-      const double* v = il + (size_t)c * FMAX;
+      double x[FMAX];
+      if (FMAX == 1)
+      {
+        x[0] = __ldg(il + c);
+      }
+      else
+      {
+        // a voxel's frames are 16-byte aligned: FMAX doubles at c * FMAX
+        const double2* v = reinterpret_cast<const double2*>(il + (size_t)c * FMAX);
+#pragma unroll
+        for (int k = 0; k < FMAX / 2; ++k)
+        {
+          const double2 q = __ldg(v + k);
+          x[2 * k] = q.x;
+          x[2 * k + 1] = q.y;
+        }
+      }
 #pragma unroll
       for (int f = 0; f < FMAX; ++f)
       {
         if (f < nf)
         {
-          const double x = __ldg(v + f);
           if (F64)
-            ld[f] = dadd(ld[f], dmul(len, x));
+            ld[f] = dadd(ld[f], dmul(len, x[f]));
           else
-            lf[f] = accumulate(lf[f], len, x);
+            lf[f] = accumulate(lf[f], len, x[f]);
         }
       }
     }
@@ -121,15 +148,43 @@ __global__ void __launch_bounds__(256) k_backward_frames(Grid g, Sino s, Tables 
   const bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
     if (inside)
     {
-#pragma unroll
-      for (int f = 0; f < FMAX; ++f)
+      if (F64 || FMAX == 1)
       {
-        if (f < nf)
+#pragma unroll
+        for (int f = 0; f < FMAX; ++f)
         {
-          if (F64)
-            atomicAdd(static_cast<double*>(acc) + (size_t)c * FMAX + f, dmul(len, v[f]));
-          else
-            atomicAdd(static_cast<float*>(acc) + (size_t)c * FMAX + f, __double2float_rn(dmul(len, v[f])));
+          if (f < nf)
+          {
+            if (F64)
+              atomicAdd(static_cast<double*>(acc) + (size_t)c * FMAX + f, dmul(len, v[f]));
+            else
+              atomicAdd(static_cast<float*>(acc) + (size_t)c * FMAX + f, __double2float_rn(dmul(len, v[f])));
+          }
+        }
+      }
+      else
+      {
+        // vector reductions: one L2 atomic for the 2 or 4 frames.  Each element
+        // still receives float(len * value); padding frames (f >= nf, value
+        // 0) receive 0 in slots nothing reads.
+        float q[FMAX];
+#pragma unroll
+        for (int f = 0; f < FMAX; ++f)
+        {
+          q[f] = __double2float_rn(dmul(len, v[f]));
+        }
+        float* a = static_cast<float*>(acc) + (size_t)c * FMAX;
+        if (FMAX == 2)
+        {
+          red_add_v2(a, q[0], q[1]);
+        }
+        else
+        {
+#pragma unroll
+          for (int k = 0; k < FMAX / 4; ++k)
+          {
+            red_add_v4(a + 4 * k, q[4 * k], q[4 * k + 1], q[4 * k + 2], q[4 * k + 3]);
+          }
         }
       }
     }
@@ -200,7 +255,7 @@ void bwd(const Grid& g, const Sino& s, const Tables& t, const void* sino, int nf
 
 int frames_stride(int nf)
 {
-  return nf <= 1 ? 1 : (nf <= 2 ? 2 : (nf <= 4 ? 4 : kMaxFramesPerPass));
+  return nf <= 1 ? 1 : (nf <= 2 ? 2 : kMaxFramesPerPass);
 }
 
 void launch_interleave(long long nvox, int nf, const void* img, bool f64, double* il, const LaunchCfg& cfg)
@@ -236,7 +291,6 @@ void launch_forward_frames(const Grid& g, const Sino& s, const Tables& t, const 
   {
     case 1: fwd<1>(g, s, t, il, nf, n_bins, out, f64, cfg); break;
     case 2: fwd<2>(g, s, t, il, nf, n_bins, out, f64, cfg); break;
-    case 4: fwd<4>(g, s, t, il, nf, n_bins, out, f64, cfg); break;
     default: fwd<kMaxFramesPerPass>(g, s, t, il, nf, n_bins, out, f64, cfg); break;
   }
 }
@@ -252,7 +306,6 @@ void launch_backward_frames(const Grid& g, const Sino& s, const Tables& t, const
   {
     case 1: bwd<1>(g, s, t, sino, nf, n_bins, acc, f64, skip_zero, cfg); break;
     case 2: bwd<2>(g, s, t, sino, nf, n_bins, acc, f64, skip_zero, cfg); break;
-    case 4: bwd<4>(g, s, t, sino, nf, n_bins, acc, f64, skip_zero, cfg); break;
     default: bwd<kMaxFramesPerPass>(g, s, t, sino, nf, n_bins, acc, f64, skip_zero, cfg); break;
   }
 }

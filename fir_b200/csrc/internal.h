@@ -154,8 +154,10 @@ void launch_batch_filter(const BatchProblem* P, const BatchItem* items, int n_it
 // Resident blocks per SM of the projector at this block size.
 int batch_max_resident(int block);
 
-// frames.cu: several frames per traversal (groups of up to kMaxFramesPerPass).
-constexpr int kMaxFramesPerPass = 8;
+// frames.cu: several frames per traversal, in groups of up to kMaxFramesPerPass
+// (measured on B200 at 8 frames of a clinical sinogram: two groups of 4 run
+// faster than one of 8, whose kernels need more registers).
+constexpr int kMaxFramesPerPass = 4;
 // Interleave stride of a group of nf frames: 1, 2, 4 or 8.
 int frames_stride(int nf);
 // il[j * stride + f] = (double) frame f of img (float or double, frame-major).

@@ -283,7 +283,7 @@ typedef enum fir_dtype
 
 /* Forward projection of the n_frames frames of vol (frame-major images) into
  * n_frames sinograms (frame-major), tracing each LOR once for a group of up to
- * 8 frames.  FIR_F32: frame f's sinogram equals fir_forward of frame f.
+ * 4 frames.  FIR_F32: frame f's sinogram equals fir_forward of frame f.
  * Counterpart: the frame loop of ForwardProj.cc:79-100 around
  * projections::forward (projections.cc:15-92). */
 fir_status fir_forward_frames(fir_ctx* ctx, const fir_vol_desc* vol, const void* img, const fir_proj_desc* proj,
