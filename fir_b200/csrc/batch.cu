@@ -49,7 +49,7 @@ __device__ __forceinline__ int take(int* queue, int grab, int lane)
 }
 
 template<bool kPersistent>
-__global__ void __launch_bounds__(256) k_batch_osem(const BatchProblem* __restrict__ P,
+__global__ void __launch_bounds__(256, 4) k_batch_osem(const BatchProblem* __restrict__ P,
                                                     const BatchItem* __restrict__ items, int n_items,
                                                     int n_bundles, int* queue, int grab, int* check)
 {

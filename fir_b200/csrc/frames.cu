@@ -33,7 +33,7 @@ __device__ __forceinline__ void red_add_v2(float* p, float a, float b)
 }
 
 template<int FMAX, bool F64>
-__global__ void __launch_bounds__(256) k_forward_frames(Grid g, Sino s, Tables t, const double* __restrict__ il,
+__global__ void __launch_bounds__(256, 4) k_forward_frames(Grid g, Sino s, Tables t, const double* __restrict__ il,
                                                         int nf, long long n_bins, void* out, int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(256) k_forward_frames(Grid g, Sino s, Tables t
 }
 
 template<int FMAX, bool F64>
-__global__ void __launch_bounds__(256) k_backward_frames(Grid g, Sino s, Tables t, const void* __restrict__ sino,
+__global__ void __launch_bounds__(256, 4) k_backward_frames(Grid g, Sino s, Tables t, const void* __restrict__ sino,
                                                          int nf, long long n_bins, void* acc, int skip_zero,
                                                          int* check)
 {

@@ -22,7 +22,7 @@ namespace
 // VolData::computeLineIntegral (VolData.cc:357-371); optional epilogue
 // ProjData::exponential (ProjData.cc:514-539).
 template<FwdEpilogue EP>
-__global__ void __launch_bounds__(256) k_forward(Grid g, Sino s, Tables t,
+__global__ void __launch_bounds__(256, 4) k_forward(Grid g, Sino s, Tables t,
                                                  const double* __restrict__ img,
                                                  float* __restrict__ sino, int* check)
 {
@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(256) k_backward(Grid g, Sino s, Tables t,
 
 // One OSEM sub-iteration over the subset of s: one thread per enumerated
 // LOR (reconAlgos.cc:119-158).
-__global__ void __launch_bounds__(256) k_osem_subset(Grid g, Sino s, Tables t,
+__global__ void __launch_bounds__(256, 4) k_osem_subset(Grid g, Sino s, Tables t,
                                                      const double* __restrict__ img,
                                                      const float* __restrict__ sino,
                                                      const float* __restrict__ bias, float* bp,

@@ -279,43 +279,108 @@ __device__ __forceinline__ bool siddon_setup(const Grid& g, const double e[6], W
 // GPU than fmin, which must also order NaNs and signed zeros).
 __device__ __forceinline__ double min_of(double a, double b) { return a < b ? a : b; }
 
-// The computePath loop (Siddon.cc:207-252).  emit(inside, linearIndex,
-// length) is called at every step; inside is FIR's checkIndices, i.e.
-// whether FIR stores the element.  Lanes with nothing to trace pass
-// go = false.  A kernel that traverses twice per lane must call __syncwarp()
-// between the traversals so that the warp enters the second one converged.
-// Returns false for a lane that hit the step bound, which only non-finite
-// input can cause.
+// The computePath loop (Siddon.cc:207-252) from the state after setup.
+//
+// FIR stores an element only while checkIndices holds (Siddon.cc:394-404)
+// and keeps stepping until alpha reaches alphaMax.  The indices start inside
+// the volume (getStartInd clamps them) and each moves monotonically, so once
+// one has left the volume no later step stores anything: the loop stops
+// there, and every step it takes stores its element.
+//
+// Tie rule (updateDim, Siddon.cc:379-392): dimension d advances when
+// |alpha_d - alphaNext| < EPS, i.e. rn(alpha_d - next) < EPS since
+// alpha_d >= next.  kFastTie uses the equivalent alpha_d < ru(next + EPS),
+// which is exact whenever next >= EPS: for next <= alpha_d <= 2 next the
+// subtraction is exact (Sterbenz), so the test is the real comparison
+// alpha_d < next + EPS, which for a double alpha_d is alpha_d < ru(next +
+// EPS); for alpha_d > 2 next both tests are false.  The fast form costs one
+// add per step instead of three.  walk_step is one step of the loop.
+// One step from prev: emits the element and advances the dimensions that
+// cross at the next alpha; returns that alpha.
+template<bool kFastTie, class Emit>
+__device__ __forceinline__ double walk_step(Walk& w, double prev, Emit&& emit)
+{
+  // MIN(alphaMax, MIN(ax, MIN(ay, az))) in FIR's order, which also fixes
+  // which operand wins when an alpha is NaN (non-finite end points).
+  const double next = min_of(w.amax, min_of(w.a[0], min_of(w.a[1], w.a[2])));
+  emit(true, w.c, dmul(dsub(next, prev), w.d12));
+  const double thr = kFastTie ? __dadd_ru(next, kEps) : 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    if (kFastTie ? w.a[d] < thr : dsub(w.a[d], next) < kEps)
+    {
+      w.a[d] = dadd(w.a[d], w.da[d]);
+      w.c += w.step[d];
+      w.left[d] -= 1;
+    }
+  }
+  return next;
+}
+
+__device__ __forceinline__ bool walk_goes_on(const Walk& w, double prev)
+{
+  return prev < w.amax && (w.left[0] | w.left[1] | w.left[2]) >= 0;
+}
+
+// With the fast tie form every alpha is finite or +inf and >= EPS, and
+// alphaMax <= 1, so every step either advances the dimension that attains
+// the minimum (using up one of its finitely many advances) or reaches
+// alphaMax: the loop ends without a step bound.  Two steps per trip.
+template<class Emit>
+__device__ __forceinline__ void walk_loop_fast(Walk& w, double& prev, bool active, Emit&& emit)
+{
+  while (active)
+  {
+    const double n1 = walk_step<true>(w, prev, emit);
+    if (!walk_goes_on(w, n1))
+    {
+      prev = n1;
+      break;
+    }
+    prev = walk_step<true>(w, n1, emit);
+    active = walk_goes_on(w, prev);
+  }
+}
+
+// The general form, bounded by the step guard (non-finite input can make a
+// step advance nothing).
+template<class Emit>
+__device__ __forceinline__ void walk_loop_exact(Walk& w, double& prev, int& guard, bool active, Emit&& emit)
+{
+  while (active)
+  {
+    prev = walk_step<false>(w, prev, emit);
+    --guard;
+    active = walk_goes_on(w, prev) && guard > 0;
+  }
+}
+
+// emit(inside, linearIndex, length) is called for every element FIR stores
+// (inside is always true; the parameter keeps the emitters' form).  Lanes
+// with nothing to trace pass go = false.  All lanes of the warp must call
+// this together (it votes on the tie form); a kernel that traverses twice
+// per lane calls __syncwarp() between the traversals.  Returns false for a
+// lane that hit the step bound, which only non-finite input can cause.
 template<class Emit>
 __device__ __forceinline__ bool siddon_walk(const Grid& g, Walk w, bool go, Emit&& emit)
 {
   double prev = w.amin;
   int guard = g.guard;
-  bool active = go && prev < w.amax;
-  while (active)
+  const bool active = go && prev < w.amax;
+  // every alpha of the walk is >= the smallest initial one (alphas only
+  // grow, alphaMax > alphaMin), so this decides the tie form for the walk
+  const bool fast = !active || min_of(w.amin, min_of(w.a[0], min_of(w.a[1], w.a[2]))) >= kEps;
+  if (__all_sync(__activemask(), fast))
   {
-    // MIN(alphaMax, MIN(ax, MIN(ay, az))) in FIR's order, which also fixes
-    // which operand wins when an alpha is NaN (non-finite end points).
-    const double next = min_of(w.amax, min_of(w.a[0], min_of(w.a[1], w.a[2])));
-    const bool inside = (w.left[0] | w.left[1] | w.left[2]) >= 0;
-    emit(inside, w.c, dmul(dsub(next, prev), w.d12));
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-    {
-      // a >= next, so |a - next| < EPS is a - next < EPS (updateDim, Siddon.cc:379-392)
-      if (dsub(w.a[d], next) < kEps)
-      {
-        w.a[d] = dadd(w.a[d], w.da[d]);
-        w.c += w.step[d];
-        w.left[d] -= 1;
-      }
-    }
-    prev = next;
-    --guard;
-    active = prev < w.amax && guard > 0;
+    walk_loop_fast(w, prev, active, emit);
   }
-  // a lane stopped by the bound still has prev < amax
-  return !go || !(prev < w.amax);
+  else
+  {
+    walk_loop_exact(w, prev, guard, active, emit);
+  }
+  // stopped by the bound: still inside, before alphaMax
+  return !go || !(prev < w.amax) || (w.left[0] | w.left[1] | w.left[2]) < 0;
 }
 
 // VolData::computeLineIntegral accumulation step (VolData.cc:362-368): the
