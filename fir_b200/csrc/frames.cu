@@ -21,15 +21,17 @@ namespace fir
 namespace
 {
 // Vector float reductions in global memory (sm_90 and later); the address
-// is 16-byte (v4) or 8-byte (v2) aligned.
+// is 16-byte (v4) or 8-byte (v2) aligned and converted to the global space.
 __device__ __forceinline__ void red_add_v4(float* p, float a, float b, float c, float d)
 {
-  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(__cvta_generic_to_global(p)), "f"(a), "f"(b),
+               "f"(c), "f"(d)
+               : "memory");
 }
 
 __device__ __forceinline__ void red_add_v2(float* p, float a, float b)
 {
-  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b) : "memory");
+  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(__cvta_generic_to_global(p)), "f"(a), "f"(b) : "memory");
 }
 
 template<int FMAX, bool F64>

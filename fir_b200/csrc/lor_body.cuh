@@ -27,6 +27,10 @@ __device__ __forceinline__ void osem_lor(const Grid& g, const Sino& s, int subse
                                          const float* __restrict__ bias, float* bp, bool skip_zero, int i,
                                          int* check)
 {
+  // bp may come from a descriptor in memory, not a kernel parameter: without
+  // this the compiler cannot tell the atomic's address space and tests it at
+  // every step.
+  __builtin_assume(__isGlobal(bp));
   const bool valid = i < s.n_enum;
   Lor l{};
   Walk w{};
