@@ -298,11 +298,25 @@ __device__ __forceinline__ double min_of(double a, double b) { return a < b ? a 
 // One step from prev: emits the element and advances the dimensions that
 // cross at the next alpha; returns that alpha.
 template<bool kFastTie, class Emit>
-__device__ __forceinline__ double walk_step(Walk& w, double prev, Emit&& emit)
+__device__ __forceinline__ double walk_step(Walk& w, double prev, bool& more, Emit&& emit)
 {
-  // MIN(alphaMax, MIN(ax, MIN(ay, az))) in FIR's order, which also fixes
-  // which operand wins when an alpha is NaN (non-finite end points).
-  const double next = min_of(w.amax, min_of(w.a[0], min_of(w.a[1], w.a[2])));
+  double next;
+  if (kFastTie)
+  {
+    // No alpha is NaN here, so MIN's operand order does not matter, and
+    // next < alphaMax (the loop test on the new prev) is the compare that
+    // picks next: m when m < alphaMax, else alphaMax.
+    const double m = min_of(w.a[0], min_of(w.a[1], w.a[2]));
+    more = m < w.amax;
+    next = more ? m : w.amax;
+  }
+  else
+  {
+    // MIN(alphaMax, MIN(ax, MIN(ay, az))) in FIR's order, which also fixes
+    // which operand wins when an alpha is NaN (non-finite end points).
+    next = min_of(w.amax, min_of(w.a[0], min_of(w.a[1], w.a[2])));
+    more = next < w.amax;
+  }
   emit(true, w.c, dmul(dsub(next, prev), w.d12));
   const double thr = kFastTie ? __dadd_ru(next, kEps) : 0.0;
 #pragma unroll
@@ -315,12 +329,8 @@ __device__ __forceinline__ double walk_step(Walk& w, double prev, Emit&& emit)
       w.left[d] -= 1;
     }
   }
+  more = more && (w.left[0] | w.left[1] | w.left[2]) >= 0;
   return next;
-}
-
-__device__ __forceinline__ bool walk_goes_on(const Walk& w, double prev)
-{
-  return prev < w.amax && (w.left[0] | w.left[1] | w.left[2]) >= 0;
 }
 
 // With the fast tie form every alpha is finite or +inf and >= EPS, and
@@ -330,16 +340,16 @@ __device__ __forceinline__ bool walk_goes_on(const Walk& w, double prev)
 template<class Emit>
 __device__ __forceinline__ void walk_loop_fast(Walk& w, double& prev, bool active, Emit&& emit)
 {
-  while (active)
+  bool more = active;
+  while (more)
   {
-    const double n1 = walk_step<true>(w, prev, emit);
-    if (!walk_goes_on(w, n1))
+    const double n1 = walk_step<true>(w, prev, more, emit);
+    if (!more)
     {
       prev = n1;
       break;
     }
-    prev = walk_step<true>(w, n1, emit);
-    active = walk_goes_on(w, prev);
+    prev = walk_step<true>(w, n1, more, emit);
   }
 }
 
@@ -348,11 +358,12 @@ __device__ __forceinline__ void walk_loop_fast(Walk& w, double& prev, bool activ
 template<class Emit>
 __device__ __forceinline__ void walk_loop_exact(Walk& w, double& prev, int& guard, bool active, Emit&& emit)
 {
-  while (active)
+  bool more = active;
+  while (more)
   {
-    prev = walk_step<false>(w, prev, emit);
+    prev = walk_step<false>(w, prev, more, emit);
     --guard;
-    active = walk_goes_on(w, prev) && guard > 0;
+    more = more && guard > 0;
   }
 }
 
