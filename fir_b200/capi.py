@@ -113,6 +113,8 @@ _SIGS = {
                                         C.c_int, C.c_int]),
     "fir_osem": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.c_void_p, C.c_void_p, C.POINTER(VolDesc),
                            C.c_void_p, C.c_void_p, C.POINTER(OsemParamsDesc), C.c_void_p, C.c_void_p]),
+    "fir_osem_psf": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.c_void_p, C.c_void_p, C.POINTER(VolDesc),
+                               C.c_void_p, C.c_void_p, C.POINTER(OsemParamsDesc), C.c_void_p, C.c_void_p]),
     "fir_osem_subiteration_noalloc": (C.c_int, [C.POINTER(ProjDesc), C.c_void_p, C.c_void_p, C.c_void_p,
                                                 C.c_void_p, C.POINTER(VolDesc), C.c_void_p, C.c_void_p,
                                                 C.POINTER(OsemParamsDesc), C.c_int, C.c_int, C.c_int,
@@ -388,8 +390,10 @@ class Context:
                                            int(subset), int(subiter)))
 
     def osem(self, proj: ProjSpec, sino, vol: VolSpec, img, sens, params: OSEMParams, bias=None,
-             save=None) -> None:
-        """``save(subiter, image_numpy)`` is called at the save interval."""
+             save=None, psf: bool = False) -> None:
+        """reconAlgos::OSEM (``psf``: the resolution-modelling form,
+        ``fir_osem_psf``).  ``save(subiter, image_numpy)`` is called at the
+        save interval."""
         self._prep(sino, img, sens, bias)
         nb = proj_geometry(proj)["n_bins"]
         cb = None
@@ -401,10 +405,11 @@ class Context:
                 save(int(subiter), arr)
 
             cb = SAVE_FN(_cb)
-        _check(lib().fir_osem(self._h, C.byref(proj_desc(proj)), _ptr(sino, n=nb), _ptr(bias, n=nb),
-                              C.byref(vol_desc(vol, 1)), _ptr(img, writable=True, n=vol.n_voxels),
-                              _ptr(sens, n=vol.n_voxels * params.n_subsets), C.byref(osem_desc(params)),
-                              C.cast(cb, C.c_void_p) if cb is not None else None, None))
+        fn = lib().fir_osem_psf if psf else lib().fir_osem
+        _check(fn(self._h, C.byref(proj_desc(proj)), _ptr(sino, n=nb), _ptr(bias, n=nb),
+                  C.byref(vol_desc(vol, 1)), _ptr(img, writable=True, n=vol.n_voxels),
+                  _ptr(sens, n=vol.n_voxels * params.n_subsets), C.byref(osem_desc(params)),
+                  C.cast(cb, C.c_void_p) if cb is not None else None, None))
 
     def ratio_backprojection(self, proj: ProjSpec, sino, vol: VolSpec, img, bp, n_subsets: int = 1,
                              subset: int = 0, bias=None) -> None:

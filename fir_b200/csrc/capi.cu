@@ -15,6 +15,8 @@
 #include "../../include/fir_cuda.h"
 #include "internal.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -62,9 +64,18 @@ void cuda_ok(cudaError_t e, const char* what)
   }
 }
 
-template<typename F>
-fir_status guarded(F&& f)
+// An NVTX range named after the ABI function brackets every call, so that
+// profilers show the host-side structure around the kernels.
+struct NvtxRange
 {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
+
+template<typename F>
+fir_status guarded(const char* name, F&& f)
+{
+  const NvtxRange range(name);
   try
   {
     f();
@@ -482,7 +493,7 @@ struct fir_ctx
   DevBuf check;     // device check word
   int* check_host = nullptr;  // pinned mirror
 
-  DevBuf bp, conv1, conv2, conv_copy, mu, wide, det, det_pairs, ratio, frames_il, frames_acc;
+  DevBuf bp, conv1, conv2, conv_copy, mu, wide, det, det_pairs, ratio, frames_il, frames_acc, psf_blur, psf_sens;
   std::vector<DevBuf> staging;
 
   // projector-kernel timing (FIR_OPT_TIMING)
@@ -942,6 +953,97 @@ void osem_subiteration_device(fir_ctx& c, const ProjInfo& p, const Tables& t, co
   cut_device(c, v, img, prm->cut_radius, 1);
 }
 
+// One sub-iteration of the resolution-modelling OSEM: the Gaussian B of the
+// parameters is part of the system model (projection of B x, B applied to
+// the backprojection, sens_frame already blurred).
+void osem_psf_subiteration_device(fir_ctx& c, const ProjInfo& p, const Tables& t, const Grid& g,
+                                  const VolInfo& v, const float* sino, const float* bias, float* img,
+                                  const float* sens_frame, const fir_osem_params* prm, int subset, int subiter)
+{
+  const size_t bytes = (size_t)v.nvox * sizeof(float);
+  float* bp = static_cast<float*>(c.bp.ensure(bytes));
+  float* blur = static_cast<float*>(c.psf_blur.ensure(bytes));
+  cuda_ok(cudaMemsetAsync(bp, 0, bytes, c.stream), "cudaMemsetAsync");
+  cuda_ok(cudaMemcpyAsync(blur, img, bytes, cudaMemcpyDeviceToDevice, c.stream), "cudaMemcpyAsync");
+  convolve_device(c, v, blur, prm->fwhm_xyz, prm->cut_radius);
+  const Sino s = sino_of(p, prm->n_subsets, subset);
+  const double* wimg = widen(c, blur, v.nvox);
+  ratio_backproject(c, g, s, t, wimg, sino, bias, bp, v.nvox);
+  convolve_device(c, v, bp, prm->fwhm_xyz, prm->cut_radius);
+  launch_em_update(v.nvox, img, bp, sens_frame, cfg_of(c));
+  after_launch(c);
+  const bool conv = prm->convolution_interval > 0 && prm->fwhm_xyz[0] > 0.0 && prm->fwhm_xyz[1] > 0.0 &&
+                    prm->fwhm_xyz[2] > 0.0;
+  if (conv && subiter % prm->convolution_interval == 0)
+  {
+    convolve_device(c, v, img, prm->fwhm_xyz, prm->cut_radius);
+  }
+  cut_device(c, v, img, prm->cut_radius, 1);
+}
+
+// The OSEM driver of fir_osem and fir_osem_psf (psf: resolution modelling).
+void osem_run(fir_ctx& c, const fir_proj_desc* proj, const float* sino, const float* bias, const fir_vol_desc* vol,
+              float* img, const float* sens, const fir_osem_params* params, fir_osem_save_fn save, void* user,
+              bool psf)
+{
+  const ProjInfo p = check_proj(proj);
+  check_osem_params(params, p);
+  const VolInfo v = check_vol(vol);
+  check_frames(v, 1);
+  const Tables t = tables_of(c, p);
+  const Grid g = grid_of(c, v);
+  if (sino == nullptr || sens == nullptr || img == nullptr)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "sinogram, image and sensitivity must not be NULL");
+  }
+  Stager st(c);
+  const float* dsino = st.in(sino, p.g.n_bins);
+  const float* dbias = st.in(bias, p.g.n_bins);
+  const float* dsens = st.in(sens, v.nvox * params->n_subsets);
+  float* dimg = st.inout(img, v.nvox);
+  if (psf)
+  {
+    // every subset's sensitivity frame blurred once: B A_s^T 1
+    const size_t sbytes = (size_t)v.nvox * params->n_subsets * sizeof(float);
+    float* sb = static_cast<float*>(c.psf_sens.ensure(sbytes));
+    cuda_ok(cudaMemcpyAsync(sb, dsens, sbytes, cudaMemcpyDeviceToDevice, c.stream), "cudaMemcpyAsync");
+    VolInfo frames = v;
+    frames.d.n_frames = params->n_subsets;
+    convolve_device(c, frames, sb, params->fwhm_xyz, params->cut_radius);
+    dsens = sb;
+  }
+  std::vector<float> host_copy;
+  cut_device(c, v, dimg, params->cut_radius, 1);
+  const int nsub_total = params->n_iterations * params->n_subsets;
+  for (int iter = 0; iter < params->n_iterations; ++iter)
+  {
+    for (int subset = 0; subset < params->n_subsets; ++subset)
+    {
+      const int subiter = iter * params->n_subsets + subset + 1;
+      const float* sframe = dsens + (size_t)subset * v.nvox;
+      if (psf)
+      {
+        osem_psf_subiteration_device(c, p, t, g, v, dsino, dbias, dimg, sframe, params, subset, subiter);
+      }
+      else
+      {
+        osem_subiteration_device(c, p, t, g, v, dsino, dbias, dimg, sframe, params, subset, subiter);
+      }
+      if (save != nullptr && params->save_interval > 0 && subiter % params->save_interval == 0 &&
+          subiter != nsub_total)
+      {
+        host_copy.resize((size_t)v.nvox);
+        cuda_ok(cudaMemcpyAsync(host_copy.data(), dimg, (size_t)v.nvox * sizeof(float), cudaMemcpyDeviceToHost,
+                                c.stream),
+                "cudaMemcpyAsync");
+        cuda_ok(cudaStreamSynchronize(c.stream), "cudaStreamSynchronize");
+        save(user, subiter, host_copy.data());
+      }
+    }
+  }
+  finish(c, st);
+}
+
 }  // namespace
 
 // ================================================================== ABI
@@ -969,7 +1071,7 @@ const char* fir_status_string(fir_status s)
 
 fir_status fir_proj_geometry(const fir_proj_desc* desc, fir_proj_info* geom, int* n_axial)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     const ProjInfo p = check_proj(desc);
     if (geom != nullptr)
     {
@@ -985,7 +1087,7 @@ fir_status fir_proj_geometry(const fir_proj_desc* desc, fir_proj_info* geom, int
 fir_status fir_scanner_tables(const fir_scanner_desc* desc, double* xy, double* z, int* n_rings,
                               int* n_crystals_per_ring)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     const ScannerInfo s = scanner_tables(desc, xy != nullptr || z != nullptr);
     if (n_rings != nullptr)
     {
@@ -1008,7 +1110,7 @@ fir_status fir_scanner_tables(const fir_scanner_desc* desc, double* xy, double* 
 
 fir_status fir_ctx_create(fir_ctx** out, int device)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     if (out == nullptr)
     {
       fail(FIR_ERR_INVALID_ARGUMENT, "output pointer is NULL");
@@ -1041,7 +1143,7 @@ fir_status fir_ctx_create(fir_ctx** out, int device)
 
 fir_status fir_ctx_destroy(fir_ctx* c)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     if (c == nullptr)
     {
       return;
@@ -1049,7 +1151,7 @@ fir_status fir_ctx_destroy(fir_ctx* c)
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     for (DevBuf* b : {&c->xy, &c->z, &c->check, &c->bp, &c->conv1, &c->conv2, &c->conv_copy, &c->mu, &c->wide,
-                      &c->det, &c->det_pairs, &c->ratio, &c->frames_il, &c->frames_acc})
+                      &c->det, &c->det_pairs, &c->ratio, &c->frames_il, &c->frames_acc, &c->psf_blur, &c->psf_sens})
     {
       b->release();
     }
@@ -1076,12 +1178,12 @@ fir_status fir_ctx_destroy(fir_ctx* c)
 
 fir_status fir_ctx_set_stream(fir_ctx* ctx, void* stream)
 {
-  return guarded([&] { check_ctx(ctx).stream = static_cast<cudaStream_t>(stream); });
+  return guarded(__func__, [&] { check_ctx(ctx).stream = static_cast<cudaStream_t>(stream); });
 }
 
 fir_status fir_ctx_set_option(fir_ctx* ctx, fir_option opt, int value)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     switch (opt)
     {
@@ -1132,7 +1234,7 @@ fir_status fir_ctx_set_option(fir_ctx* ctx, fir_option opt, int value)
 
 fir_status fir_ctx_projector_time(fir_ctx* ctx, double* ms, long long* launches, int reset)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     drain_timing(c);
     if (ms != nullptr)
@@ -1153,7 +1255,7 @@ fir_status fir_ctx_projector_time(fir_ctx* ctx, double* ms, long long* launches,
 
 fir_status fir_ctx_get_option(fir_ctx* ctx, fir_option opt, int* value)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     if (value == nullptr)
     {
@@ -1174,7 +1276,7 @@ fir_status fir_ctx_get_option(fir_ctx* ctx, fir_option opt, int* value)
 
 fir_status fir_ctx_set_scanner(fir_ctx* ctx, const fir_scanner_desc* scanner)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const ScannerInfo s = scanner_tables(scanner, true);
     cuda_ok(cudaStreamSynchronize(c.stream), "cudaStreamSynchronize");
@@ -1190,7 +1292,7 @@ fir_status fir_ctx_set_scanner(fir_ctx* ctx, const fir_scanner_desc* scanner)
 
 fir_status fir_ctx_synchronize(fir_ctx* ctx)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     read_checks(c);
   });
@@ -1201,7 +1303,7 @@ long long fir_ctx_launch_count(const fir_ctx* ctx) { return ctx != nullptr ? ctx
 fir_status fir_forward(fir_ctx* ctx, const fir_vol_desc* vol, const float* img, const fir_proj_desc* proj,
                        float* sino)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const VolInfo v = check_vol(vol);
     const ProjInfo p = check_proj(proj);
@@ -1220,7 +1322,7 @@ fir_status fir_forward(fir_ctx* ctx, const fir_vol_desc* vol, const float* img, 
 fir_status fir_forward_exp(fir_ctx* ctx, const fir_vol_desc* vol, const float* mu, const fir_proj_desc* proj,
                            float* acf)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const VolInfo v = check_vol(vol);
     const ProjInfo p = check_proj(proj);
@@ -1239,7 +1341,7 @@ fir_status fir_forward_exp(fir_ctx* ctx, const fir_vol_desc* vol, const float* m
 fir_status fir_backward(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const fir_vol_desc* vol,
                         float* img, int n_subsets)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const ProjInfo p = check_proj(proj);
     check_subsets(p, n_subsets);
@@ -1283,7 +1385,7 @@ static bool check_dtype(fir_dtype d)
 fir_status fir_forward_frames(fir_ctx* ctx, const fir_vol_desc* vol, const void* img, const fir_proj_desc* proj,
                               void* sino, fir_dtype dtype)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const VolInfo v = check_vol(vol);
     const ProjInfo p = check_proj(proj);
@@ -1317,7 +1419,7 @@ fir_status fir_forward_frames(fir_ctx* ctx, const fir_vol_desc* vol, const void*
 fir_status fir_backward_frames(fir_ctx* ctx, const fir_proj_desc* proj, const void* sino, const fir_vol_desc* vol,
                                void* img, fir_dtype dtype)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const ProjInfo p = check_proj(proj);
     const VolInfo v = check_vol(vol);
@@ -1354,7 +1456,7 @@ fir_status fir_backward_frames(fir_ctx* ctx, const fir_proj_desc* proj, const vo
 fir_status fir_sensitivity(fir_ctx* ctx, const fir_proj_desc* proj, const fir_vol_desc* vol, float* sens,
                            int n_subsets)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const ProjInfo p = check_proj(proj);
     check_subsets(p, n_subsets);
@@ -1383,7 +1485,7 @@ fir_status fir_osem_subiteration(fir_ctx* ctx, const fir_proj_desc* proj, const 
                                  const fir_vol_desc* vol, float* img, const float* sens_frame,
                                  const fir_osem_params* params, int subset, int subiter)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const ProjInfo p = check_proj(proj);
     check_osem_params(params, p);
@@ -1413,53 +1515,25 @@ fir_status fir_osem(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, 
                     const fir_vol_desc* vol, float* img, const float* sens, const fir_osem_params* params,
                     fir_osem_save_fn save, void* user)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] { osem_run(check_ctx(ctx), proj, sino, bias, vol, img, sens, params, save, user, false); });
+}
+
+fir_status fir_osem_psf(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const float* bias,
+                        const fir_vol_desc* vol, float* img, const float* sens, const fir_osem_params* params,
+                        fir_osem_save_fn save, void* user)
+{
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
-    const ProjInfo p = check_proj(proj);
-    check_osem_params(params, p);
-    const VolInfo v = check_vol(vol);
-    check_frames(v, 1);
-    const Tables t = tables_of(c, p);
-    const Grid g = grid_of(c, v);
-    if (sino == nullptr || sens == nullptr || img == nullptr)
-    {
-      fail(FIR_ERR_INVALID_ARGUMENT, "sinogram, image and sensitivity must not be NULL");
-    }
-    Stager st(c);
-    const float* dsino = st.in(sino, p.g.n_bins);
-    const float* dbias = st.in(bias, p.g.n_bins);
-    const float* dsens = st.in(sens, v.nvox * params->n_subsets);
-    float* dimg = st.inout(img, v.nvox);
-    std::vector<float> host_copy;
-    cut_device(c, v, dimg, params->cut_radius, 1);
-    const int nsub_total = params->n_iterations * params->n_subsets;
-    for (int iter = 0; iter < params->n_iterations; ++iter)
-    {
-      for (int subset = 0; subset < params->n_subsets; ++subset)
-      {
-        const int subiter = iter * params->n_subsets + subset + 1;
-        osem_subiteration_device(c, p, t, g, v, dsino, dbias, dimg, dsens + (size_t)subset * v.nvox, params,
-                                 subset, subiter);
-        if (save != nullptr && params->save_interval > 0 && subiter % params->save_interval == 0 &&
-            subiter != nsub_total)
-        {
-          host_copy.resize((size_t)v.nvox);
-          cuda_ok(cudaMemcpyAsync(host_copy.data(), dimg, (size_t)v.nvox * sizeof(float), cudaMemcpyDeviceToHost,
-                                  c.stream),
-                  "cudaMemcpyAsync");
-          cuda_ok(cudaStreamSynchronize(c.stream), "cudaStreamSynchronize");
-          save(user, subiter, host_copy.data());
-        }
-      }
-    }
-    finish(c, st);
+    const bool psf = params != nullptr && params->fwhm_xyz[0] > 0.0f && params->fwhm_xyz[1] > 0.0f &&
+                     params->fwhm_xyz[2] > 0.0f;
+    osem_run(c, proj, sino, bias, vol, img, sens, params, save, user, psf);
   });
 }
 
 fir_status fir_ratio_backprojection(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const float* bias,
                                     const fir_vol_desc* vol, const float* img, float* bp, int n_subsets, int subset)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const ProjInfo p = check_proj(proj);
     check_subsets(p, n_subsets);
@@ -1490,7 +1564,7 @@ fir_status fir_ratio_backprojection(fir_ctx* ctx, const fir_proj_desc* proj, con
 
 fir_status fir_em_update(fir_ctx* ctx, const fir_vol_desc* vol, float* img, float* bp, const float* sens_frame)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const VolInfo v = check_vol(vol);
     Stager st(c);
@@ -1506,7 +1580,7 @@ fir_status fir_em_update(fir_ctx* ctx, const fir_vol_desc* vol, float* img, floa
 fir_status fir_convolve(fir_ctx* ctx, const fir_vol_desc* vol, float* img, const float fwhm_xyz[3],
                         float cut_radius)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const VolInfo v = check_vol(vol);
     if (fwhm_xyz == nullptr)
@@ -1522,7 +1596,7 @@ fir_status fir_convolve(fir_ctx* ctx, const fir_vol_desc* vol, float* img, const
 
 fir_status fir_cut_circle(fir_ctx* ctx, const fir_vol_desc* vol, float* img, float cut_radius)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const VolInfo v = check_vol(vol);
     Stager st(c);
@@ -1534,7 +1608,7 @@ fir_status fir_cut_circle(fir_ctx* ctx, const fir_vol_desc* vol, float* img, flo
 
 fir_status fir_apply_mask(fir_ctx* ctx, const fir_vol_desc* vol, float* img, const float* mask)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const VolInfo v = check_vol(vol);
     Stager st(c);
@@ -1548,7 +1622,7 @@ fir_status fir_apply_mask(fir_ctx* ctx, const fir_vol_desc* vol, float* img, con
 
 fir_status fir_hu_to_mu(fir_ctx* ctx, const fir_vol_desc* vol, float* img)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const VolInfo v = check_vol(vol);
     Stager st(c);
@@ -1561,7 +1635,7 @@ fir_status fir_hu_to_mu(fir_ctx* ctx, const fir_vol_desc* vol, float* img)
 
 fir_status fir_proj_exponential(fir_ctx* ctx, const fir_proj_desc* proj, float* sino)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const ProjInfo p = check_proj(proj);
     Stager st(c);
@@ -1574,7 +1648,7 @@ fir_status fir_proj_exponential(fir_ctx* ctx, const fir_proj_desc* proj, float* 
 
 fir_status fir_proj_multiply(fir_ctx* ctx, const fir_proj_desc* proj, float* a, const float* b)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const ProjInfo p = check_proj(proj);
     Stager st(c);
@@ -1589,7 +1663,7 @@ fir_status fir_proj_multiply(fir_ctx* ctx, const fir_proj_desc* proj, float* a, 
 fir_status fir_siddon_paths(fir_ctx* ctx, const fir_vol_desc* vol, long long n, const double* ends, int cap,
                             int* coords, double* lengths, int* counts, int* crosses)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const VolInfo v = check_vol(vol);
     const Grid g = grid_of(c, v);
@@ -1612,7 +1686,7 @@ fir_status fir_siddon_paths(fir_ctx* ctx, const fir_vol_desc* vol, long long n, 
 fir_status fir_lor_paths(fir_ctx* ctx, const fir_proj_desc* proj, const fir_vol_desc* vol, long long n,
                          const long long* bins, int cap, int* coords, double* lengths, int* counts, int* crosses)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_ctx& c = check_ctx(ctx);
     const ProjInfo p = check_proj(proj);
     const VolInfo v = check_vol(vol);
@@ -1842,7 +1916,7 @@ extern "C" {
 fir_status fir_batch_create(fir_batch** out, fir_ctx* ctx, int n_problems, const fir_scanner_desc* scanners,
                             const fir_proj_desc* projs, const fir_vol_desc* vols, const fir_osem_params* params)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     if (out == nullptr)
     {
       fail(FIR_ERR_INVALID_ARGUMENT, "output pointer is NULL");
@@ -2012,7 +2086,7 @@ fir_status fir_batch_create(fir_batch** out, fir_ctx* ctx, int n_problems, const
 
 fir_status fir_batch_destroy(fir_batch* batch)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     if (batch == nullptr)
     {
       return;
@@ -2032,7 +2106,7 @@ fir_status fir_batch_destroy(fir_batch* batch)
 
 fir_status fir_batch_set_data(fir_batch* batch, int p, const float* sino, const float* sens, const float* bias)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_batch& b = check_batch(batch);
     fir_batch::Problem& q = batch_problem(b, p);
     if (sino == nullptr || sens == nullptr)
@@ -2061,7 +2135,7 @@ fir_status fir_batch_set_data(fir_batch* batch, int p, const float* sino, const 
 
 fir_status fir_batch_set_image(fir_batch* batch, int p, const float* img)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_batch& b = check_batch(batch);
     fir_batch::Problem& q = batch_problem(b, p);
     if (img == nullptr)
@@ -2076,7 +2150,7 @@ fir_status fir_batch_set_image(fir_batch* batch, int p, const float* img)
 
 fir_status fir_batch_get_image(fir_batch* batch, int p, float* img)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_batch& b = check_batch(batch);
     fir_batch::Problem& q = batch_problem(b, p);
     if (img == nullptr)
@@ -2090,7 +2164,7 @@ fir_status fir_batch_get_image(fir_batch* batch, int p, float* img)
 
 fir_status fir_batch_set_launch(fir_batch* batch, int block, int blocks_per_sm, int grab)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_batch& b = check_batch(batch);
     if (block < 32 || block > 256 || block % 32 != 0)
     {
@@ -2113,7 +2187,7 @@ fir_status fir_batch_set_launch(fir_batch* batch, int block, int blocks_per_sm, 
 
 fir_status fir_batch_get_launch(const fir_batch* batch, int* block, int* blocks_per_sm, int* grab)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     if (batch == nullptr)
     {
       fail(FIR_ERR_INVALID_ARGUMENT, "batch is NULL");
@@ -2129,7 +2203,7 @@ fir_status fir_batch_get_launch(const fir_batch* batch, int* block, int* blocks_
 
 fir_status fir_batch_schedule(const fir_batch* batch, int* n_steps, long long* n_launches)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     if (batch == nullptr)
     {
       fail(FIR_ERR_INVALID_ARGUMENT, "batch is NULL");
@@ -2143,7 +2217,7 @@ fir_status fir_batch_schedule(const fir_batch* batch, int* n_steps, long long* n
 
 fir_status fir_batch_tune(fir_batch* batch, double* best_ms)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_batch& b = check_batch(batch);
     if (b.steps.empty())
     {
@@ -2223,7 +2297,7 @@ fir_status fir_batch_tune(fir_batch* batch, double* best_ms)
 
 fir_status fir_batch_osem(fir_batch* batch, int use_graph)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     fir_batch& b = check_batch(batch);
     batch_begin(b);
     if (use_graph)
@@ -2324,7 +2398,7 @@ extern "C" fir_status fir_osem_subiteration_noalloc(const fir_proj_desc* proj, c
                                                     const fir_osem_params* params, int subset, int subiter,
                                                     int geometry, void* stream)
 {
-  return guarded([&] {
+  return guarded(__func__, [&] {
     const ProjInfo p = check_proj(proj);
     check_osem_params(params, p);
     if (subset < 0 || subset >= params->n_subsets)

@@ -11,6 +11,7 @@
  *   fir_osem_subiteration  one sub-iteration of reconAlgos::OSEM  src_lib/reconAlgos.cc:119-198
  *   fir_osem               reconAlgos::OSEM                src_lib/reconAlgos.h:29-36, reconAlgos.cc:63-201
  *   fir_ratio_backprojection  the getLine/ratio/projectLineIntegral loop of OSEM and OSEM_ResoReco  src_lib/reconAlgos.cc:119-158, :273-312
+ *   fir_osem_psf              reconAlgos::OSEM_ResoReco, corrected (PSF in the model)              src_lib/reconAlgos.cc:203-367
  *   fir_convolve           operations::convolve            src_lib/operations.h:7-10, operations.cc:11-192
  *   fir_cut_circle         operations::cutCircle           src_lib/operations.h:13-15, operations.cc:194-220
  *   fir_apply_mask         operations::applyMask           src_lib/operations.h:19, operations.cc:222-241
@@ -271,6 +272,20 @@ typedef void (*fir_osem_save_fn)(void* user, int subiter, const float* img);
 fir_status fir_osem(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const float* bias,
                     const fir_vol_desc* vol, float* img, const float* sens,
                     const fir_osem_params* params, fir_osem_save_fn save, void* user);
+
+/* Resolution-modelling OSEM: the corrected form of reconAlgos::OSEM_ResoReco
+ * (reconAlgos.cc:203-367).  The Gaussian B = operations::convolve(fwhm_xyz,
+ * cut_radius) is part of the system model A B:
+ * - every sensitivity frame is blurred once, B A_s^T 1;
+ * - each sub-iteration projects B x, backprojects measured/estimated, and
+ *   blurs the backprojection before the EM update.
+ * FIR's version projects x instead of B x (reconAlgos.cc:296) and divides the
+ * image rather than the backprojection by the sensitivity (:323).  The
+ * post-filter of convolution_interval and the cut are applied as in
+ * fir_osem.  With any FWHM <= 0 this is fir_osem. */
+fir_status fir_osem_psf(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const float* bias,
+                        const fir_vol_desc* vol, float* img, const float* sens, const fir_osem_params* params,
+                        fir_osem_save_fn save, void* user);
 
 /* ---- multi-frame projection ----
  *

@@ -608,9 +608,16 @@ void fo_proj_multiply(long long n, float* a, const float* b)
 }
 
 /* ---- OSEM: reconAlgos.cc:11-59 (getLine), :63-201 (loop) ---- */
-void fo_osem(const fo_proj* p, const float* sino, const float* bias, const fo_vol* v,
-             int truncate, const double* xy, const double* z, float* img, const float* sens,
-             const fo_osem_params* prm)
+/* The OSEM loop of reconAlgos.cc:63-201.  With psf, the resolution-modelling
+ * variant that OSEM_ResoReco (reconAlgos.cc:203-367) intends, corrected: the
+ * Gaussian B = operations::convolve(fwhm, cutRadius) sits inside the system
+ * model.  Each sub-iteration projects B x (FIR projects x, :296), blurs the
+ * backprojection (:300-304), and divides it by the blurred sensitivity of
+ * the subset before the usual EM update (FIR divides the image, :323);
+ * every sensitivity frame is blurred once before the loop. */
+static void osem_loop(const fo_proj* p, const float* sino, const float* bias, const fo_vol* v, int truncate,
+                      const double* xy, const double* z, float* img, const float* sens, const fo_osem_params* prm,
+                      int psf)
 {
   fo_grid g;
   fo_grid_init(&g, v, truncate);
@@ -622,11 +629,27 @@ void fo_osem(const fo_proj* p, const float* sino, const float* bias, const fo_vo
   const int conv = prm->convolution_interval > 0 && prm->fwhm[0] > 0.0 && prm->fwhm[1] > 0.0 &&
                    prm->fwhm[2] > 0.0;
   const int nsub = prm->n_subsets, vps = p->n_views / nsub;
+  float* blur = NULL;
+  float* sens_b = NULL;
+  if (psf)
+  {
+    blur = (float*)malloc(sizeof(float) * (size_t)nvox);
+    sens_b = (float*)malloc(sizeof(float) * (size_t)(nvox * nsub));
+    memcpy(sens_b, sens, sizeof(float) * (size_t)(nvox * nsub));
+    for (int s = 0; s < nsub; ++s) fo_convolve(v, sens_b + nvox * s, prm->fwhm, prm->cut_radius);
+  }
   fo_cut_circle(v, img, prm->cut_radius);
   for (int iter = 0; iter < prm->n_iterations; ++iter)
     for (int subset = 0; subset < nsub; ++subset)
     {
       const int subiter = iter * nsub + subset + 1;
+      const float* model = img;
+      if (psf)
+      {
+        memcpy(blur, img, sizeof(float) * (size_t)nvox);
+        fo_convolve(v, blur, prm->fwhm, prm->cut_radius);
+        model = blur;
+      }
       for (int seg = -p->seg_offset; seg <= p->seg_offset; ++seg)
       {
         const int nax = p->n_axial[seg + p->seg_offset];
@@ -645,7 +668,7 @@ void fo_osem(const fo_proj* p, const float* sino, const float* bias, const fo_vo
               const int crosses = fo_siddon(&g, e[0], e[1], e[2], e[3], e[4], e[5], co, le, cap, &n);
               float line = 0.0f;
               if (crosses)
-                for (int k = 0; k < n; ++k) line = (float)((double)line + le[k] * (double)img[co[k]]);
+                for (int k = 0; k < n; ++k) line = (float)((double)line + le[k] * (double)model[co[k]]);
               if (bias) line += bias[bin];
               if ((double)line > FO_EPS)
               {
@@ -655,12 +678,28 @@ void fo_osem(const fo_proj* p, const float* sino, const float* bias, const fo_vo
             }
         }
       }
-      fo_em_update(nvox, img, bp, sens + nvox * subset);
+      if (psf) fo_convolve(v, bp, prm->fwhm, prm->cut_radius);
+      fo_em_update(nvox, img, bp, (psf ? sens_b : sens) + nvox * subset);
       if (conv && subiter % prm->convolution_interval == 0) fo_convolve(v, img, prm->fwhm, prm->cut_radius);
       fo_cut_circle(v, img, prm->cut_radius);
       memset(bp, 0, sizeof(float) * (size_t)nvox);
     }
+  free(blur);
+  free(sens_b);
   free(bp);
   free(co);
   free(le);
+}
+
+void fo_osem(const fo_proj* p, const float* sino, const float* bias, const fo_vol* v, int truncate,
+             const double* xy, const double* z, float* img, const float* sens, const fo_osem_params* prm)
+{
+  osem_loop(p, sino, bias, v, truncate, xy, z, img, sens, prm, 0);
+}
+
+void fo_osem_psf(const fo_proj* p, const float* sino, const float* bias, const fo_vol* v, int truncate,
+                 const double* xy, const double* z, float* img, const float* sens, const fo_osem_params* prm)
+{
+  const int psf = prm->fwhm[0] > 0.0 && prm->fwhm[1] > 0.0 && prm->fwhm[2] > 0.0;
+  osem_loop(p, sino, bias, v, truncate, xy, z, img, sens, prm, psf);
 }

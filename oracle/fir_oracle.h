@@ -97,6 +97,13 @@ void fo_osem(const fo_proj* p, const float* sino, const float* bias, const fo_vo
              int truncate, const double* xy, const double* z, float* img,
              const float* sens, const fo_osem_params* prm);
 
+/* Resolution-modelling OSEM with the Gaussian PSF inside the system model
+ * (the corrected OSEM_ResoReco, reconAlgos.cc:203-367); with any FWHM <= 0
+ * it is fo_osem. */
+void fo_osem_psf(const fo_proj* p, const float* sino, const float* bias, const fo_vol* v,
+                 int truncate, const double* xy, const double* z, float* img,
+                 const float* sens, const fo_osem_params* prm);
+
 void fo_em_update(long long n, float* img, float* bp, const float* sens);
 void fo_convolve(const fo_vol* v, float* img, const float* fwhm, float cut_radius);
 void fo_cut_circle(const fo_vol* v, float* img, float cut_radius);

@@ -186,3 +186,22 @@ def test_oracle_span3_and_lor_tables(restated, reference):
     for p in (ProjSpec(5, 32, 3, 8, 3), ProjSpec(9, 64, 5, 0, 3), ProjSpec(8, 128, 15, 43, 1)):
         nb = reference.proj_geometry(p)["n_bins"]
         np.testing.assert_array_equal(restated.lor_table(p), reference.lor_table(p, nb))
+
+
+def test_oracle_psf_osem_reduces_to_osem_without_psf(restated):
+    """The resolution-modelling OSEM of the restatement with FWHM 0 is
+    bit-identical to its OSEM, and with a PSF it differs."""
+    from fir_b200 import workloads
+    from fir_b200.geometry import OSEMParams
+
+    w = workloads.tiny()
+    x = workloads.activity(w)
+    y = workloads.poisson_counts(restated.forward(w.scanner, w.proj, w.vol, x), w.counts, 1)
+    sens = restated.sensitivity(w.scanner, w.proj, w.vol, 4)
+    prm0 = OSEMParams(n_iterations=1, n_subsets=4, fwhm_xyz=[0.0, 0.0, 0.0])
+    a = restated.osem(w.scanner, w.proj, w.vol, y, np.ones_like(x), sens, prm0)
+    b = restated.osem(w.scanner, w.proj, w.vol, y, np.ones_like(x), sens, prm0, psf=True)
+    np.testing.assert_array_equal(a, b)
+    prm = OSEMParams(n_iterations=1, n_subsets=4, fwhm_xyz=[4.0, 4.0, 4.0])
+    c = restated.osem(w.scanner, w.proj, w.vol, y, np.ones_like(x), sens, prm, psf=True)
+    assert np.abs(c - a).max() > 1e-3
