@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--det-steps", type=int, default=2,
                     help="extra sub-iterations timed with deterministic backprojection (0: skip)")
+    ap.add_argument("--skip-zero-steps", type=int, default=4,
+                    help="extra sub-iterations timed with FIR_OPT_SKIP_ZERO_BINS (0: skip)")
     ap.add_argument("--batch-runs", type=int, default=2,
                     help="timed runs of the 64-problem batched OSEM and of its sequential plain form (0: skip)")
     ap.add_argument("--batch-problems", type=int, default=64)
@@ -738,6 +740,33 @@ def main():
         "roofline": roofline,
         "clocks": {k2: v for k2, v in clocks.summary().items() if k2 != "samples"},
     }
+
+    # ---- the same steps skipping bins with no counts (exact: their ratio is 0),
+    # reported beside the headline, which traces every bin as FIR does
+    if args.skip_zero_steps > 0:
+        ctx.set_option(capi.FIR_OPT_SKIP_ZERO_BINS, 1)
+        sz_ms, sz_steps = 0.0, 0
+        for _ in range(args.skip_zero_steps):
+            s = k % nsub
+            sz_steps += s_fwd[s] + s_bwd(s)
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step(s, k + 1)
+            b.record(stream)
+            torch.cuda.synchronize()
+            sz_ms += a.elapsed_time(b)
+            k += 1
+        ctx.set_option(capi.FIR_OPT_SKIP_ZERO_BINS, 0)
+        result["skip_zero_bins"] = {
+            "value": sz_steps / (sz_ms / 1000.0),
+            "unit": UNIT,
+            "ms_per_step": sz_ms / args.skip_zero_steps,
+            "steps": args.skip_zero_steps,
+            "zero_bin_fraction": float((y == 0).float().mean()),
+            "note": "FIR_OPT_SKIP_ZERO_BINS: bins with y = 0 are not traced (their ratio is exactly 0); steps "
+                    "counted as for the headline",
+        }
 
     # ---- the same steps with deterministic backprojection (FIR's serial order)
     if args.det_steps > 0:

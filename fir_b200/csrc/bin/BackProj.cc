@@ -1,6 +1,7 @@
 // FIR_BackProj <projection .hs> <scanner file> <volume template .h33> <output name>
 // Backprojection of a sinogram into a single-frame volume (FIR:
 // src_bin/BackProj.cc).  All four arguments are required.
+#include <runtime.h>
 #include <ProjData.h>
 #include <ScannerData.h>
 #include <VolData.h>
@@ -26,5 +27,6 @@ int main(int argc, char** argv)
     std::cerr << ex.what();
     return EXIT_FAILURE;
   }
+  fir_runtime::reportTiming("FIR_BackProj");
   return EXIT_SUCCESS;
 }

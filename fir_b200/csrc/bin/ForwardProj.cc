@@ -10,6 +10,7 @@
 //   !END OF FORWARD PROJECTION PARAMETERS :=
 // With several frames (or an explicit frame list) the outputs are
 // <name>_frame_<k>.
+#include <runtime.h>
 #include <KeyParser.h>
 #include <ProjData.h>
 #include <ScannerData.h>
@@ -102,5 +103,6 @@ int main(int argc, char** argv)
     std::cerr << ex.what();
     return EXIT_FAILURE;
   }
+  fir_runtime::reportTiming("FIR_ForwardProj");
   return EXIT_SUCCESS;
 }

@@ -17,6 +17,7 @@
 //   attenuation correction factors := <name> (read if present, else computed and written)
 //   !END OF OSEM PARAMETERS :=
 // A flag that does not start with '0' means "recompute" (both default to 1).
+#include <runtime.h>
 #include <KeyParser.h>
 #include <ProjData.h>
 #include <ScannerData.h>
@@ -172,5 +173,6 @@ int main(int argc, char** argv)
     std::cerr << ex.what();
     return EXIT_FAILURE;
   }
+  fir_runtime::reportTiming("FIR_OSEM");
   return EXIT_SUCCESS;
 }

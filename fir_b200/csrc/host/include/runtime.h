@@ -20,6 +20,10 @@ fir_ctx* context();
 void useScanner(const ScannerData& scanner);
 // Throws on a non-OK status.
 void check(fir_status status, const char* what);
+// With FIR_TIMING_JSON set (not "0") when the context was created: prints
+// one JSON line to stderr with the wall time since then, the device time and
+// number of projector launches, and the number of kernel launches.
+void reportTiming(const char* program);
 
 fir_vol_desc volDesc(const VolData& vol, int nFrames);
 fir_proj_desc projDesc(const ProjData& proj);

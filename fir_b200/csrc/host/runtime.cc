@@ -5,6 +5,8 @@
 #include <console.h>
 #include <runtime.h>
 
+#include <chrono>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -16,6 +18,8 @@ struct Holder
   fir_ctx* ctx = nullptr;
   bool haveScanner = false;
   fir_scanner_desc scanner{};
+  bool timing = false;
+  std::chrono::steady_clock::time_point start;
 
   ~Holder()
   {
@@ -45,6 +49,15 @@ fir_ctx* context()
   {
     const char* dev = std::getenv("FIR_DEVICE");
     check(fir_ctx_create(&g_holder.ctx, dev ? std::atoi(dev) : 0), "creating the GPU context");
+    g_holder.start = std::chrono::steady_clock::now();
+    if (const char* t = std::getenv("FIR_TIMING_JSON"))
+    {
+      if (std::strcmp(t, "0") != 0)
+      {
+        check(fir_ctx_set_option(g_holder.ctx, FIR_OPT_TIMING, 1), "FIR_TIMING_JSON");
+        g_holder.timing = true;
+      }
+    }
     if (const char* g = std::getenv("FIR_GEOMETRY"))
     {
       if (std::strcmp(g, "exact") == 0)
@@ -54,6 +67,23 @@ fir_ctx* context()
     }
   }
   return g_holder.ctx;
+}
+
+void reportTiming(const char* program)
+{
+  if (!g_holder.timing || g_holder.ctx == nullptr)
+  {
+    return;
+  }
+  double ms = 0.0;
+  long long n = 0;
+  check(fir_ctx_projector_time(g_holder.ctx, &ms, &n, 0), "timing");
+  const double wall =
+    std::chrono::duration<double>(std::chrono::steady_clock::now() - g_holder.start).count();
+  std::fprintf(stderr,
+               "{\"program\": \"%s\", \"wall_s\": %.6f, \"projector_ms\": %.3f, \"projector_launches\": %lld, "
+               "\"kernel_launches\": %lld}\n",
+               program, wall, ms, n, fir_ctx_launch_count(g_holder.ctx));
 }
 
 void useScanner(const ScannerData& scanner)

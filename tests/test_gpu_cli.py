@@ -34,13 +34,14 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-def run(bindir, exe, *args, cwd):
+def run(bindir, exe, *args, cwd, extra_env=None):
     path = os.path.join(bindir, exe)
     if not os.access(path, os.X_OK):
         pytest.skip(f"{path} not built")
-    env = dict(os.environ, OMP_NUM_THREADS="1")
+    env = dict(os.environ, OMP_NUM_THREADS="1", **(extra_env or {}))
     p = subprocess.run([path, *args], capture_output=True, text=True, cwd=cwd, env=env, timeout=600)
     assert p.returncode == 0, f"{path}: {p.stdout[-2000:]}{p.stderr[-2000:]}"
+    return p
 
 
 @pytest.fixture(scope="module")
@@ -152,3 +153,19 @@ def test_osem_with_attenuation_matches_fir(files):
     first = np.fromfile(d / "rec_ours.i33", np.float32)
     run(OURS, "FIR_OSEM", osem_params(d, "ours"), "0", "0", cwd=d)
     assert rel_l2(np.fromfile(d / "rec_ours.i33", np.float32), first) <= 1e-6
+
+
+def test_timing_json_line(files):
+    """FIR_TIMING_JSON=1 makes our executables print one JSON timing line on
+    stderr; without it they print none."""
+    import json
+
+    d, w, x = files
+    p = run(OURS, "FIR_ForwardProj", fwd_params(d, "t_json", "image.h33"), cwd=d, extra_env={"FIR_TIMING_JSON": "1"})
+    lines = [ln for ln in p.stderr.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, p.stderr
+    rec = json.loads(lines[0])
+    assert rec["program"] == "FIR_ForwardProj"
+    assert rec["projector_launches"] >= 1 and rec["projector_ms"] > 0 and rec["kernel_launches"] >= 1
+    q = run(OURS, "FIR_ForwardProj", fwd_params(d, "t_nojson", "image.h33"), cwd=d)
+    assert not [ln for ln in q.stderr.splitlines() if ln.startswith("{")]
