@@ -136,6 +136,9 @@ _SIGS = {
                                      C.c_int]),
     "fir_backward_frames": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.c_void_p, C.POINTER(VolDesc), C.c_void_p,
                                       C.c_int]),
+    "fir_bin_coordinates": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.c_longlong, C.c_void_p, C.c_void_p,
+                                      C.c_void_p]),
+    "fir_proj_rebin_weight": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.c_void_p]),
     "fir_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_void_p, C.c_int, C.POINTER(ScannerDesc),
                                    C.POINTER(ProjDesc), C.POINTER(VolDesc), C.POINTER(OsemParamsDesc)]),
     "fir_batch_destroy": (C.c_int, [C.c_void_p]),
@@ -481,6 +484,24 @@ class Context:
         self._prep(img, sino)
         vd, pi, ps, dt = self._frames_args(vol, img, proj, sino)
         _check(lib().fir_backward_frames(self._h, C.byref(proj_desc(proj)), ps, C.byref(vd), pi, dt))
+
+    def bin_coordinates(self, proj: ProjSpec, pairs):
+        """ProjData::getBinCoordinates of n (ring1, crystal1, ring2, crystal2)
+        pairs: returns (coords [n, 5] = found, seg, view, axial, tang; bins [n]
+        flat index or -1)."""
+        pairs = np.ascontiguousarray(np.asarray(pairs, np.int32).reshape(-1, 4))
+        n = pairs.shape[0]
+        coords = np.zeros((n, 5), np.int32)
+        bins = np.zeros(n, np.int64)
+        _check(lib().fir_bin_coordinates(self._h, C.byref(proj_desc(proj)), n, pairs.ctypes.data,
+                                         coords.ctypes.data, bins.ctypes.data))
+        return coords, bins
+
+    def proj_rebin_weight(self, proj: ProjSpec, sino) -> None:
+        """ProjData::rebinWeight in place."""
+        self._prep(sino)
+        nb = proj_geometry(proj)["n_bins"]
+        _check(lib().fir_proj_rebin_weight(self._h, C.byref(proj_desc(proj)), _ptr(sino, writable=True, n=nb)))
 
     def siddon_paths(self, vol: VolSpec, ends, cap: Optional[int] = None):
         ends = np.ascontiguousarray(ends, np.float64).reshape(-1, 6)

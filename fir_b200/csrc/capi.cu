@@ -18,6 +18,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -493,7 +494,7 @@ struct fir_ctx
   DevBuf check;     // device check word
   int* check_host = nullptr;  // pinned mirror
 
-  DevBuf bp, conv1, conv2, conv_copy, mu, wide, det, det_pairs, ratio, frames_il, frames_acc, psf_blur, psf_sens;
+  DevBuf bp, conv1, conv2, conv_copy, mu, wide, det, det_pairs, ratio, frames_il, frames_acc, psf_blur, psf_sens, rebin;
   std::vector<DevBuf> staging;
 
   // projector-kernel timing (FIR_OPT_TIMING)
@@ -1151,7 +1152,7 @@ fir_status fir_ctx_destroy(fir_ctx* c)
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     for (DevBuf* b : {&c->xy, &c->z, &c->check, &c->bp, &c->conv1, &c->conv2, &c->conv_copy, &c->mu, &c->wide,
-                      &c->det, &c->det_pairs, &c->ratio, &c->frames_il, &c->frames_acc, &c->psf_blur, &c->psf_sens})
+                      &c->det, &c->det_pairs, &c->ratio, &c->frames_il, &c->frames_acc, &c->psf_blur, &c->psf_sens, &c->rebin})
     {
       b->release();
     }
@@ -1657,6 +1658,126 @@ fir_status fir_proj_multiply(fir_ctx* ctx, const fir_proj_desc* proj, float* a, 
     launch_proj_multiply(p.g.n_bins, da, db, cfg_of(c));
     after_launch(c);
     finish(c, st);
+  });
+}
+
+// The (segment, axial) factors of ProjData::rebinWeight (ProjData.cc:541-615),
+// one float per row of a span > 1 sinogram, 1 where FIR leaves the row
+// alone: the ring differences of one ring sum are walked from the most
+// negative, grouped into the segments' bands, and a band that merges w > 1
+// of them gets (float)(1.0 / w).  FIR writes these rows through
+// ProjData::weightBin, whose index adds the segment offset twice
+// (ProjData.inl:76-79 with ProjHeader.inl:55) and leaves the arrays once
+// there is more than one segment; here each factor goes to the row the
+// algorithm names.
+static std::vector<float> rebin_factors(const ProjInfo& p, int max_axial)
+{
+  const int ns = p.d.n_segments, span = p.d.segment_span, nr = p.d.n_rings;
+  const int seg_off = p.g.seg_offset, mrd = p.g.max_ring_diff;
+  std::vector<float> t((size_t)ns * max_axial, 1.0f);
+  std::vector<char> hit((size_t)ns * max_axial, 0);
+  for (int rs = 0; rs <= 2 * (nr - 1); ++rs)
+  {
+    int lmd = std::min(rs <= nr - 1 ? rs : 2 * (nr - 1) - rs, mrd);
+    if ((rs + lmd) % 2 != 0)
+    {
+      --lmd;
+    }
+    int seg = -seg_off - 1;
+    int next = -mrd - 1;
+    while (next < -lmd)
+    {
+      ++seg;
+      next += span;
+    }
+    int w = 1;
+    for (int rd = -lmd; rd <= lmd; rd += 2)
+    {
+      if (rd == lmd || rd + 1 >= next)
+      {
+        if (w > 1)
+        {
+          const int aseg = seg < 0 ? -seg : seg;
+          const int ax = seg == 0 ? rs : rs - (span + 1) / 2 - (aseg - 1) * span;
+          const int si = seg + seg_off;
+          if (si < 0 || si >= ns || ax < 0 || ax >= p.n_axial[(size_t)si])
+          {
+            fail(FIR_ERR_NOT_SUPPORTED, "rebin weight row (segment ", seg, ", axial ", ax, ") outside the sinogram");
+          }
+          const size_t k = (size_t)si * max_axial + ax;
+          if (hit[k])
+          {
+            fail(FIR_ERR_NOT_SUPPORTED, "rebin weight row (segment ", seg, ", axial ", ax, ") weighted twice");
+          }
+          hit[k] = 1;
+          t[k] = (float)(1.0 / w);
+        }
+        w = 1;
+        ++seg;
+        next += span;
+      }
+      else
+      {
+        ++w;
+      }
+    }
+  }
+  return t;
+}
+
+fir_status fir_bin_coordinates(fir_ctx* ctx, const fir_proj_desc* proj, long long n, const int* pairs, int* coords,
+                               long long* bins)
+{
+  return guarded(__func__, [&] {
+    fir_ctx& c = check_ctx(ctx);
+    const ProjInfo p = check_proj(proj);
+    if (n < 0 || (n > 0 && pairs == nullptr))
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "n must be >= 0 and pairs non-NULL");
+    }
+    if (n == 0)
+    {
+      return;
+    }
+    Stager st(c);
+    const int* dpairs = st.in(pairs, 4 * n);
+    int* dcoords = st.out(coords, 5 * n);
+    long long* dbins = st.out(bins, n);
+    if (reinterpret_cast<uintptr_t>(dpairs) % 16 != 0)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "device crystal pairs must be 16-byte aligned");
+    }
+    launch_bin_coordinates(sino_of(p, 1, 0), p.g.max_ring_diff, n, dpairs, dcoords, dbins, cfg_of(c));
+    after_launch(c);
+    finish(c, st);
+  });
+}
+
+fir_status fir_proj_rebin_weight(fir_ctx* ctx, const fir_proj_desc* proj, float* sino)
+{
+  return guarded(__func__, [&] {
+    fir_ctx& c = check_ctx(ctx);
+    const ProjInfo p = check_proj(proj);
+    if (sino == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "sinogram is NULL");
+    }
+    if (p.d.segment_span == 1)
+    {
+      return;  // ProjData.cc:543: nothing to do for span 1
+    }
+    const int max_axial = *std::max_element(p.n_axial.begin(), p.n_axial.end());
+    const std::vector<float> table = rebin_factors(p, max_axial);
+    Stager st(c);
+    float* dsino = st.inout(sino, p.g.n_bins);
+    float* dtable = static_cast<float*>(c.rebin.ensure(table.size() * sizeof(float)));
+    cuda_ok(cudaMemcpyAsync(dtable, table.data(), table.size() * sizeof(float), cudaMemcpyHostToDevice, c.stream),
+            "cudaMemcpyAsync");
+    launch_rebin_weight(sino_of(p, 1, 0), dtable, max_axial, dsino, cfg_of(c));
+    after_launch(c);
+    finish(c, st);
+    // the table is pageable host memory: keep it until the copy is done
+    cuda_ok(cudaStreamSynchronize(c.stream), "cudaStreamSynchronize");
   });
 }
 

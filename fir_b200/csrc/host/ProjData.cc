@@ -266,3 +266,28 @@ void ProjData::exponential()
   const fir_proj_desc d = fir_runtime::projDesc(*this);
   fir_runtime::check(fir_proj_exponential(fir_runtime::context(), &d, mData.data()), "ProjData::exponential");
 }
+
+bool ProjData::getBinCoordinates(int crystalAxialCoord1, int crystalAngCoord1, int crystalAxialCoord2,
+                                 int crystalAngCoord2, int* seg, int* view, int* axialCoord, int* tangCoord) const
+{
+  const fir_proj_desc d = fir_runtime::projDesc(*this);
+  const int pair[4] = {crystalAxialCoord1, crystalAngCoord1, crystalAxialCoord2, crystalAngCoord2};
+  int coords[5] = {0, 0, 0, 0, 0};
+  fir_runtime::check(fir_bin_coordinates(fir_runtime::context(), &d, 1, pair, coords, nullptr),
+                     "ProjData::getBinCoordinates");
+  if (coords[0] == 0)
+  {
+    return false;
+  }
+  *seg = coords[1];
+  *view = coords[2];
+  *axialCoord = coords[3];
+  *tangCoord = coords[4];
+  return true;
+}
+
+void ProjData::rebinWeight()
+{
+  const fir_proj_desc d = fir_runtime::projDesc(*this);
+  fir_runtime::check(fir_proj_rebin_weight(fir_runtime::context(), &d, mData.data()), "ProjData::rebinWeight");
+}

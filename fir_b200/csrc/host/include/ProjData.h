@@ -79,9 +79,16 @@ public:
   std::tuple<int, int> getCrystalAxialCoord(int seg, int axialCoord) const;
   std::tuple<int, int> getCrystalAngCoord(int view, int tangCoord) const;
 
-  // Bin-wise arithmetic on the GPU: product with 1e-5 gates, exponential
+  // Crystal pair -> bin coordinates (ProjData.cc:342-479); false when the LOR
+  // lies outside the allocated segments or tangential range.
+  bool getBinCoordinates(int crystalAxialCoord1, int crystalAngCoord1, int crystalAxialCoord2, int crystalAngCoord2,
+                         int* seg, int* view, int* axialCoord, int* tangCoord) const;
+
+  // Bin-wise arithmetic on the GPU: product with 1e-5 gates, exponential,
+  // and the span > 1 weights of ProjData.cc:541-615
   ProjData& operator*=(const ProjData& inputProj);
   void exponential();
+  void rebinWeight();
 
   const ProjHeader& getHeader() const { return mHeader; }
   const ProjGeometry& getGeometry() const { return mGeometry; }

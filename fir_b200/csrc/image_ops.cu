@@ -171,6 +171,61 @@ __global__ void k_proj_multiply(long long n, float* a, const float* __restrict__
     a[i] = ((double)x > kEps && (double)y > kEps) ? __fmul_rn(x, y) : 0.0f;
   }
 }
+// ProjData::getBinCoordinates on n crystal pairs; coords[5i..] = FIR's
+// result flag, seg, view, axial, tang (zeros where the flag is 0), bins[i] =
+// flat file-order
+// index, or -1 where FIR returns false or the coordinates fall outside the
+// sinogram's arrays.
+__global__ void k_bin_coordinates(Sino s, int max_ring_diff, long long n, const int4* __restrict__ pairs,
+                                  int* coords, long long* bins)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n)
+  {
+    return;
+  }
+  const int4 q = pairs[i];
+  int c[4] = {0, 0, 0, 0};
+  const bool ok = bin_of_crystals(s, max_ring_diff, q.x, q.y, q.z, q.w, c);
+  long long flat = -1;
+  if (ok)
+  {
+    const int si = c[0] + s.seg_offset;
+    if (si >= 0 && si < s.n_segments && c[1] >= 0 && c[1] < s.n_views && c[2] >= 0 && c[2] < s.n_axial[si])
+    {
+      flat = (long long)s.seg_base[si] + ((long long)c[1] * s.n_axial[si] + c[2]) * s.n_tang + c[3] + s.tang_offset;
+    }
+  }
+  if (coords != nullptr)
+  {
+    coords[5 * i] = ok ? 1 : 0;
+    coords[5 * i + 1] = ok ? c[0] : 0;
+    coords[5 * i + 2] = ok ? c[1] : 0;
+    coords[5 * i + 3] = ok ? c[2] : 0;
+    coords[5 * i + 4] = ok ? c[3] : 0;
+  }
+  if (bins != nullptr)
+  {
+    bins[i] = flat;
+  }
+}
+
+// ProjData::rebinWeight: bin *= factor of its (segment, axial) row, for the
+// rows whose factor is not 1 (table: n_segments x max_axial floats).
+__global__ void k_rebin_weight(Sino s, const float* __restrict__ table, int max_axial, float* sino)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n_enum)
+  {
+    return;
+  }
+  const Lor l = decode_bin(s, i);
+  const float f = __ldg(table + (l.seg + s.seg_offset) * max_axial + l.axial);
+  if (f != 1.0f)
+  {
+    sino[l.bin] = __fmul_rn(sino[l.bin], f);
+  }
+}
 }  // namespace
 
 void launch_em_update(long long n, float* img, float* bp, const float* sens, const LaunchCfg& cfg)
@@ -248,6 +303,24 @@ void launch_proj_multiply(long long n, float* a, const float* b, const LaunchCfg
   if (n > 0)
   {
     k_proj_multiply<<<blocks_for(n), kBlock, 0, cfg.stream>>>(n, a, b);
+  }
+}
+
+void launch_bin_coordinates(const Sino& s, int max_ring_diff, long long n, const int* pairs, int* coords,
+                            long long* bins, const LaunchCfg& cfg)
+{
+  if (n > 0)
+  {
+    k_bin_coordinates<<<blocks_for(n), kBlock, 0, cfg.stream>>>(s, max_ring_diff, n,
+                                                                reinterpret_cast<const int4*>(pairs), coords, bins);
+  }
+}
+
+void launch_rebin_weight(const Sino& s, const float* table, int max_axial, float* sino, const LaunchCfg& cfg)
+{
+  if (s.n_enum > 0)
+  {
+    k_rebin_weight<<<blocks_for(s.n_enum), kBlock, 0, cfg.stream>>>(s, table, max_axial, sino);
   }
 }
 }  // namespace fir

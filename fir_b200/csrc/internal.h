@@ -81,6 +81,13 @@ void launch_apply_mask(long long n, float* img, const float* mask, const LaunchC
 void launch_hu_to_mu(long long n, float* img, const LaunchCfg& cfg);
 void launch_exponential(long long n, float* sino, const LaunchCfg& cfg);
 void launch_proj_multiply(long long n, float* a, const float* b, const LaunchCfg& cfg);
+// ProjData::getBinCoordinates on n (ring1, crystal1, ring2, crystal2) int4
+// pairs (16-byte aligned); coords (5 ints per pair: flag, seg, view, axial,
+// tang) and bins may be nullptr.
+void launch_bin_coordinates(const Sino& s, int max_ring_diff, long long n, const int* pairs, int* coords,
+                            long long* bins, const LaunchCfg& cfg);
+// sino *= table[segment][axial] where the factor is not 1 (s: one subset).
+void launch_rebin_weight(const Sino& s, const float* table, int max_axial, float* sino, const LaunchCfg& cfg);
 
 // Distance of voxel (x, y)'s centre from the volume axis, in FIR's double
 // arithmetic (operations.cc:160-185 and :206-212).

@@ -175,6 +175,59 @@ __device__ __forceinline__ void lor_ends(const Sino& s, const Tables& t, const L
   e[5] = __ldg(t.z + a2);
 }
 
+// ProjData::getBinCoordinates (ProjData.cc:342-479): the bin (seg, view,
+// axial, tang) of the LOR between crystal c1 of ring r1 and crystal c2 of
+// ring r2; false when the LOR lies outside the allocated segments or
+// tangential range.  Integer arithmetic with truncating division, as FIR's.
+__device__ __forceinline__ bool bin_of_crystals(const Sino& s, int max_ring_diff, int r1, int c1, int r2, int c2,
+                                                int out[4])
+{
+  const int n = s.n_cpr;
+  int aseg = r1 > r2 ? r1 - r2 : r2 - r1;
+  if (aseg > max_ring_diff)
+  {
+    return false;
+  }
+  const int sum = c1 + c2;
+  const int s1 = (sum >= n / 2 && sum < 3 * n / 2) ? -1 : 1;
+  const int t = s1 * ((c2 > c1 ? c2 - c1 : c1 - c2) - n / 2);
+  if (t < -s.tang_offset || t >= -s.tang_offset + s.n_tang)
+  {
+    return false;
+  }
+  int ax;
+  if (s.span == 1)
+  {
+    ax = (r1 + r2 - aseg) / 2;
+  }
+  else
+  {
+    const bool central = aseg <= s.half_span;
+    aseg = central ? 0 : 1 + (aseg - s.half_span - 1) / s.span;
+    const int m = central ? 0 : 1 + s.half_span + (aseg - 1) * s.span;
+    ax = r1 + r2 - m;
+  }
+  int seg = aseg;
+  if (seg != 0)
+  {
+    // the crystals of the parallel LOR nearest the axis (tang 0 or 1) decide
+    // the sign together with the ring order
+    const int s2 = c1 < c2 ? 1 : -1;
+    const int at = t < 0 ? -t : t;
+    const int u = at % 2 == 0 ? -t / 2 : -(t - 1) / 2;
+    int k1 = c1 - s1 * s2 * u;
+    int k2 = c2 + s1 * s2 * u;
+    k1 = k1 >= n ? k1 - n : (k1 < 0 ? k1 + n : k1);
+    k2 = k2 >= n ? k2 - n : (k2 < 0 ? k2 + n : k2);
+    seg = seg * (r1 < r2 ? -1 : 1) * (k1 < k2 ? 1 : -1);
+  }
+  out[0] = seg;
+  out[1] = ((sum + n / 2) % n) / 2;
+  out[2] = ax;
+  out[3] = t;
+  return true;
+}
+
 // State of one path.  The voxel is tracked as its linear index plus, per
 // dimension, the number of further advances that keep the index inside the
 // volume: FIR's checkIndices (Siddon.cc:394-404) holds exactly while all

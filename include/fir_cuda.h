@@ -18,6 +18,8 @@
  *   fir_hu_to_mu           operations::HounsfieldToMuMap   src_lib/operations.h:22, operations.cc:243-284
  *   fir_proj_exponential   ProjData::exponential           src_lib/ProjData.h:108, ProjData.cc:514-539
  *   fir_proj_multiply      ProjData::operator*=            src_lib/ProjData.h:107, ProjData.cc:481-512
+ *   fir_bin_coordinates    ProjData::getBinCoordinates     src_lib/ProjData.h:96-104, ProjData.cc:342-479
+ *   fir_proj_rebin_weight  ProjData::rebinWeight           src_lib/ProjData.h:112, ProjData.cc:541-615
  *   fir_em_update          VolData /=, *= of the EM update src_lib/VolData.cc:305-343, reconAlgos.cc:161-166
  *   fir_lor_paths          Siddon::computePathBetweenCrystals (path dump) src_lib/Siddon.cc:88-258
  *   fir_siddon_paths       Siddon::computePath (path dump) src_lib/Siddon.h:45-55
@@ -372,6 +374,24 @@ fir_status fir_apply_mask(fir_ctx* ctx, const fir_vol_desc* vol, float* img, con
 fir_status fir_hu_to_mu(fir_ctx* ctx, const fir_vol_desc* vol, float* img);
 fir_status fir_proj_exponential(fir_ctx* ctx, const fir_proj_desc* proj, float* sino);
 fir_status fir_proj_multiply(fir_ctx* ctx, const fir_proj_desc* proj, float* a, const float* b);
+
+/* ProjData::getBinCoordinates (ProjData.h:96-104, ProjData.cc:342-479) for n
+ * LORs.  pairs: n x (ring1, crystal1, ring2, crystal2) ints (a device pointer
+ * must be 16-byte aligned).  coords (may be NULL): n x (found, seg, view,
+ * axial, tang), found being FIR's return value and the rest zeros where it
+ * is 0.  bins (may be NULL): the flat
+ * file-order bin index, or -1 where FIR returns false or the coordinates
+ * fall outside the sinogram's arrays. */
+fir_status fir_bin_coordinates(fir_ctx* ctx, const fir_proj_desc* proj, long long n, const int* pairs, int* coords,
+                               long long* bins);
+/* ProjData::rebinWeight (ProjData.h:112, ProjData.cc:541-615), in place: for
+ * span > 1, every bin of an axial position that merges w > 1 ring
+ * differences of one ring sum is multiplied by (float)(1.0 / w); span 1 is a
+ * no-op.  FIR indexes these rows through ProjData::getInd, which adds the
+ * segment offset twice (ProjData.inl:76-79, ProjHeader.inl:55) and writes
+ * outside its arrays once there is more than one segment; here every row the
+ * algorithm names is weighted. */
+fir_status fir_proj_rebin_weight(fir_ctx* ctx, const fir_proj_desc* proj, float* sino);
 
 /* ---- path dumps (debugging and parity checks) ---- */
 /* Siddon::computePath for n segments, ends[6*i..6*i+5] = (x1,y1,z1,x2,y2,z2).

@@ -135,6 +135,8 @@ class Restated:
         L.fo_osem.argtypes = [C.POINTER(FoProj), _f32p, C.c_void_p, C.POINTER(FoVol), C.c_int, _f64p, _f64p,
                               _f32p, _f32p, C.POINTER(FoOsem)]
         L.fo_osem_psf.argtypes = L.fo_osem.argtypes
+        L.fo_bin_coordinates.argtypes = [C.POINTER(FoProj)] + [C.c_int] * 4 + [C.POINTER(C.c_int)] * 4
+        L.fo_rebin_weight.argtypes = [C.POINTER(FoProj), _f32p]
         L.fo_em_update.argtypes = [C.c_longlong, _f32p, _f32p, _f32p]
         L.fo_convolve.argtypes = [C.POINTER(FoVol), _f32p, _f32p, C.c_float]
         L.fo_cut_circle.argtypes = [C.POINTER(FoVol), _f32p, C.c_float]
@@ -249,6 +251,23 @@ class Restated:
            np.ascontiguousarray(sens, np.float32).ravel(), C.byref(o))
         return img.reshape(v.shape_zyx)
 
+    def bin_coordinates(self, p: ProjSpec, pairs):
+        """[n, 5]: flag, seg, view, axial, tang of each (ring1, crystal1,
+        ring2, crystal2) pair (zeros where the flag is 0)."""
+        f = self.proj(p)
+        pairs = np.asarray(pairs, np.int64).reshape(-1, 4)
+        out = np.zeros((pairs.shape[0], 5), np.int32)
+        o = [C.c_int() for _ in range(4)]
+        for i, (r1, c1, r2, c2) in enumerate(pairs):
+            if self.L.fo_bin_coordinates(C.byref(f), int(r1), int(c1), int(r2), int(c2), *[C.byref(x) for x in o]):
+                out[i] = (1, o[0].value, o[1].value, o[2].value, o[3].value)
+        return out
+
+    def rebin_weight(self, p: ProjSpec, sino):
+        out = np.ascontiguousarray(sino, np.float32).copy()
+        self.L.fo_rebin_weight(C.byref(self.proj(p)), out)
+        return out
+
     def em_update(self, img, bp, sens):
         img = np.ascontiguousarray(img, np.float32).copy()
         bp = np.ascontiguousarray(bp, np.float32).copy()
@@ -329,6 +348,8 @@ class Reference:
         L.ref_hu_to_mu.argtypes = [C.POINTER(RefVol), _f32p]
         L.ref_proj_exponential.argtypes = [C.c_char_p, _f32p]
         L.ref_proj_multiply.argtypes = [C.c_char_p, _f32p, _f32p]
+        L.ref_bin_coordinates.argtypes = [C.c_char_p, C.c_longlong, C.c_void_p, C.c_void_p]
+        L.ref_rebin_weight.argtypes = [C.c_char_p, _f32p]
         L.ref_em_update.argtypes = [C.POINTER(RefVol), _f32p, _f32p, _f32p]
         self.tmp = tempfile.mkdtemp(prefix="firref_")
         self._n = 0
@@ -459,6 +480,19 @@ class Reference:
         _, hp = self._files(None, p)
         out = np.ascontiguousarray(a, np.float32).copy()
         self._check(self.L.ref_proj_multiply(hp, out, np.ascontiguousarray(b, np.float32)))
+        return out
+
+    def bin_coordinates(self, p: ProjSpec, pairs):
+        _, hp = self._files(None, p)
+        pairs = np.ascontiguousarray(np.asarray(pairs, np.int32).reshape(-1, 4))
+        out = np.zeros((pairs.shape[0], 5), np.int32)
+        self._check(self.L.ref_bin_coordinates(hp, pairs.shape[0], pairs.ctypes.data, out.ctypes.data))
+        return out
+
+    def rebin_weight(self, p: ProjSpec, sino):
+        _, hp = self._files(None, p)
+        out = np.ascontiguousarray(sino, np.float32).copy()
+        self._check(self.L.ref_rebin_weight(hp, out))
         return out
 
     def em_update(self, v: VolSpec, img, bp, sens):

@@ -703,3 +703,94 @@ void fo_osem_psf(const fo_proj* p, const float* sino, const float* bias, const f
   const int psf = prm->fwhm[0] > 0.0 && prm->fwhm[1] > 0.0 && prm->fwhm[2] > 0.0;
   osem_loop(p, sino, bias, v, truncate, xy, z, img, sens, prm, psf);
 }
+
+/* ProjData::getBinCoordinates (ProjData.cc:342-479): the sinogram bin of the
+ * LOR between (ring1, crystal1) and (ring2, crystal2), in integer arithmetic
+ * with C's truncating division.  Returns 0 when the LOR lies outside the
+ * allocated segments or tangential range. */
+int fo_bin_coordinates(const fo_proj* p, int r1, int c1, int r2, int c2, int* seg, int* view, int* axial,
+                       int* tang)
+{
+  const int n = p->n_crystals_per_ring;
+  int aseg = r1 > r2 ? r1 - r2 : r2 - r1;
+  if (aseg > p->max_ring_diff) return 0;
+  const int sum = c1 + c2;
+  const int s1 = (sum >= n / 2 && sum < 3 * n / 2) ? -1 : 1;
+  const int t = s1 * ((c2 > c1 ? c2 - c1 : c1 - c2) - n / 2);
+  if (t < -p->tang_offset || t >= -p->tang_offset + p->n_tang_coords) return 0;
+  int ax;
+  if (p->segment_span == 1)
+    ax = (r1 + r2 - aseg) / 2;
+  else
+  {
+    const int central = aseg <= p->half_span;
+    aseg = central ? 0 : 1 + (aseg - p->half_span - 1) / p->segment_span;
+    const int m = central ? 0 : 1 + p->half_span + (aseg - 1) * p->segment_span;
+    ax = r1 + r2 - m;
+  }
+  const int v = ((sum + n / 2) % n) / 2;
+  int sg = aseg;
+  if (sg != 0)
+  {
+    const int s2 = c1 < c2 ? 1 : -1;
+    const int at = t < 0 ? -t : t;
+    const int u = at % 2 == 0 ? -t / 2 : -(t - 1) / 2;
+    int k1 = c1 - s1 * s2 * u, k2 = c2 + s1 * s2 * u;
+    if (k1 >= n) k1 -= n; else if (k1 < 0) k1 += n;
+    if (k2 >= n) k2 -= n; else if (k2 < 0) k2 += n;
+    sg = sg * (r1 < r2 ? -1 : 1) * (k1 < k2 ? 1 : -1);
+  }
+  *seg = sg;
+  *view = v;
+  *axial = ax;
+  *tang = t;
+  return 1;
+}
+
+/* ProjData::rebinWeight (ProjData.cc:541-615): for span > 1, every bin of an
+ * axial position that merges w > 1 ring differences of one ring sum is
+ * multiplied by (float)(1.0 / w), serially in FIR's loop order. */
+void fo_rebin_weight(const fo_proj* p, float* sino)
+{
+  if (p->segment_span == 1) return;
+  const int nr = p->n_rings, span = p->segment_span;
+  for (int rs = 0; rs <= 2 * (nr - 1); ++rs)
+  {
+    int lmd = rs <= nr - 1 ? rs : 2 * (nr - 1) - rs;
+    if (lmd > p->max_ring_diff) lmd = p->max_ring_diff;
+    if ((rs + lmd) % 2) --lmd;
+    int seg = -p->seg_offset - 1, next = -p->max_ring_diff - 1;
+    while (next < -lmd)
+    {
+      ++seg;
+      next += span;
+    }
+    int w = 1;
+    for (int rd = -lmd; rd <= lmd; rd += 2)
+    {
+      if (rd == lmd || rd + 1 >= next)
+      {
+        if (w > 1)
+        {
+          const int aseg = seg < 0 ? -seg : seg;
+          const int ax = seg == 0 ? rs : rs - (span + 1) / 2 - (aseg - 1) * span;
+          const float f = (float)(1.0 / w);
+          const int nax = p->n_axial[seg + p->seg_offset];
+          const long long bpv = (long long)nax * p->n_tang_coords;
+          const long long base = seg_base(p, seg);
+          for (int view = 0; view < p->n_views; ++view)
+            for (int ti = 0; ti < p->n_tang_coords; ++ti)
+            {
+              const long long bin = base + view * bpv + (long long)ax * p->n_tang_coords + ti;
+              sino[bin] = sino[bin] * f;
+            }
+        }
+        w = 1;
+        ++seg;
+        next += span;
+      }
+      else
+        ++w;
+    }
+  }
+}

@@ -105,6 +105,12 @@ void fo_osem_psf(const fo_proj* p, const float* sino, const float* bias, const f
                  const float* sens, const fo_osem_params* prm);
 
 void fo_em_update(long long n, float* img, float* bp, const float* sens);
+
+/* ProjData::getBinCoordinates: 1 and the bin of the crystal pair, or 0. */
+int fo_bin_coordinates(const fo_proj* p, int r1, int c1, int r2, int c2, int* seg, int* view, int* axial,
+                       int* tang);
+/* ProjData::rebinWeight on a flat sinogram (no-op for span 1). */
+void fo_rebin_weight(const fo_proj* p, float* sino);
 void fo_convolve(const fo_vol* v, float* img, const float* fwhm, float cut_radius);
 void fo_cut_circle(const fo_vol* v, float* img, float cut_radius);
 void fo_apply_mask(long long n, float* img, const float* mask);

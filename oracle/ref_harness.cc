@@ -512,6 +512,43 @@ int ref_proj_multiply(const char* projHeader, float* a, const float* b)
     });
 }
 
+// ProjData::getBinCoordinates (ProjData.cc:342-479) on n crystal pairs
+// (ring1, crystal1, ring2, crystal2): out[5i] = returned flag, then seg,
+// view, axial, tang (0 where FIR returns false).
+int ref_bin_coordinates(const char* projHeader, long long n, const int* pairs, int* out)
+{
+  return guarded(
+    [&]
+    {
+      ProjData proj(projHeader, ProjData::ConstructionMode::ALLOCATE);
+      for (long long i = 0; i < n; ++i)
+      {
+        int seg = 0, view = 0, axial = 0, tang = 0;
+        const bool ok =
+          proj.getBinCoordinates(pairs[4 * i], pairs[4 * i + 1], pairs[4 * i + 2], pairs[4 * i + 3], &seg, &view,
+                                 &axial, &tang);
+        out[5 * i] = ok ? 1 : 0;
+        out[5 * i + 1] = ok ? seg : 0;
+        out[5 * i + 2] = ok ? view : 0;
+        out[5 * i + 3] = ok ? axial : 0;
+        out[5 * i + 4] = ok ? tang : 0;
+      }
+    });
+}
+
+// ProjData::rebinWeight (ProjData.cc:541-615) applied to sino in place.
+int ref_rebin_weight(const char* projHeader, float* sino)
+{
+  return guarded(
+    [&]
+    {
+      ProjData proj(projHeader, ProjData::ConstructionMode::ALLOCATE);
+      projIn(proj, sino);
+      proj.rebinWeight();
+      projOut(proj, sino);
+    });
+}
+
 // Element-wise EM image update of reconAlgos.cc:161-166, via VolData's own
 // operators (VolData.cc:305-343): bp /= sens; img *= bp.
 int ref_em_update(const ref_vol* v, float* img, float* bp, const float* sens)

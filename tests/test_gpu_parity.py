@@ -370,3 +370,75 @@ def test_osem_psf_matches_oracle(gpu_ctx_factory, restated):
     ctx.osem(w.proj, y, w.vol, a, sens, prm0, psf=True)
     ctx.osem(w.proj, y, w.vol, b, sens, prm0)
     assert rel_l2(a, b) <= 1e-5
+
+
+# ------------------------------------------- bin coordinates, rebin weights
+
+BIN_HEADERS = [
+    ProjSpec(8, 128, 15, 43),
+    ProjSpec(8, 128, 9, 0),
+    ProjSpec(8, 128, 5, 61, 3),
+    ProjSpec(8, 96, 3, 0, 5),
+    ProjSpec(9, 64, 3, 21, 3),
+    ProjSpec(32, 512, 21, 125, 3),
+]
+
+
+def flat_bins(restated, p, coords):
+    f = restated.proj(p)
+    nax = np.array(f.n_axial[:p.n_segments], np.int64)
+    bpv = nax * f.n_tang_coords
+    base = np.concatenate([[0], np.cumsum(bpv * f.n_views)])
+    si = coords[:, 1] + f.seg_offset
+    ok = (coords[:, 0] == 1) & (si >= 0) & (si < p.n_segments)
+    si = np.where(ok, si, 0)
+    ok &= (coords[:, 2] >= 0) & (coords[:, 2] < f.n_views) & (coords[:, 3] >= 0) & (coords[:, 3] < nax[si])
+    flat = base[si] + coords[:, 2] * bpv[si] + coords[:, 3] * f.n_tang_coords + coords[:, 4] + f.tang_offset
+    return np.where(ok, flat, -1)
+
+
+@pytest.mark.parametrize("k", range(len(BIN_HEADERS)))
+def test_bin_coordinates_match_oracle(gpu_ctx_factory, restated, k):
+    """fir_bin_coordinates equals the restatement of getBinCoordinates (itself
+    pinned to compiled FIR) on random crystal pairs, flag and coordinates;
+    the flat index is that of the coordinates."""
+    p = BIN_HEADERS[k]
+    rng = np.random.default_rng(40 + k)
+    n = 50000
+    pairs = np.stack([rng.integers(0, p.n_rings, n), rng.integers(0, p.n_crystals_per_ring, n),
+                      rng.integers(0, p.n_rings, n), rng.integers(0, p.n_crystals_per_ring, n)], axis=1)
+    coords, bins = gpu_ctx_factory().bin_coordinates(p, pairs)
+    want = restated.bin_coordinates(p, pairs)
+    np.testing.assert_array_equal(coords, want)
+    np.testing.assert_array_equal(bins, flat_bins(restated, p, want))
+
+
+def test_bin_coordinates_invert_the_bin_to_crystal_map(gpu_ctx_factory, restated):
+    """Span 1, clinical header: the crystal pair of a bin (getCrystalAxialCoord,
+    getCrystalAngCoord; rings = slices / 2) maps back to the same bin."""
+    p = workloads.clinical().proj
+    n = capi.proj_geometry(p)["n_bins"]
+    bins = np.sort(np.random.default_rng(3).choice(n, 20000, replace=False))
+    t = restated.lor_table_bins(p, bins)
+    pairs = np.stack([t[:, 0] // 2, t[:, 1], t[:, 2] // 2, t[:, 3]], axis=1)
+    coords, got = gpu_ctx_factory().bin_coordinates(p, pairs)
+    assert (coords[:, 0] == 1).all()
+    np.testing.assert_array_equal(got, bins)
+
+
+@pytest.mark.parametrize("k", range(len(BIN_HEADERS)))
+def test_rebin_weight_matches_oracle(gpu_ctx_factory, restated, torch, k):
+    """fir_proj_rebin_weight equals the restatement bit for bit, on host and
+    device buffers (no-op for span 1)."""
+    p = BIN_HEADERS[k]
+    n = capi.proj_geometry(p)["n_bins"]
+    sino = (np.random.default_rng(k).random(n) * 100).astype(np.float32)
+    want = restated.rebin_weight(p, sino)
+    ctx = gpu_ctx_factory()
+    got = sino.copy()
+    ctx.proj_rebin_weight(p, got)
+    np.testing.assert_array_equal(got, want)
+    dev = torch.from_numpy(sino).cuda()
+    ctx.proj_rebin_weight(p, dev)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(dev.cpu().numpy(), want)
