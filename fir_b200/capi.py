@@ -115,6 +115,9 @@ _SIGS = {
                            C.c_void_p, C.c_void_p, C.POINTER(OsemParamsDesc), C.c_void_p, C.c_void_p]),
     "fir_osem_psf": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.c_void_p, C.c_void_p, C.POINTER(VolDesc),
                                C.c_void_p, C.c_void_p, C.POINTER(OsemParamsDesc), C.c_void_p, C.c_void_p]),
+    "fir_osem_weighted": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.POINTER(VolDesc), C.c_void_p, C.c_void_p, C.POINTER(OsemParamsDesc),
+                                    C.c_void_p, C.c_void_p]),
     "fir_osem_subiteration_noalloc": (C.c_int, [C.POINTER(ProjDesc), C.c_void_p, C.c_void_p, C.c_void_p,
                                                 C.c_void_p, C.POINTER(VolDesc), C.c_void_p, C.c_void_p,
                                                 C.POINTER(OsemParamsDesc), C.c_int, C.c_int, C.c_int,
@@ -393,11 +396,12 @@ class Context:
                                            int(subset), int(subiter)))
 
     def osem(self, proj: ProjSpec, sino, vol: VolSpec, img, sens, params: OSEMParams, bias=None,
-             save=None, psf: bool = False) -> None:
+             save=None, psf: bool = False, mult=None) -> None:
         """reconAlgos::OSEM (``psf``: the resolution-modelling form,
-        ``fir_osem_psf``).  ``save(subiter, image_numpy)`` is called at the
-        save interval."""
-        self._prep(sino, img, sens, bias)
+        ``fir_osem_psf``; ``mult``: per-bin multiplicative factors of the
+        ordinary-Poisson model, ``fir_osem_weighted``, with sens = A_s^T mult).
+        ``save(subiter, image_numpy)`` is called at the save interval."""
+        self._prep(sino, img, sens, bias, mult)
         nb = proj_geometry(proj)["n_bins"]
         cb = None
         if save is not None:
@@ -408,6 +412,15 @@ class Context:
                 save(int(subiter), arr)
 
             cb = SAVE_FN(_cb)
+        if mult is not None:
+            if psf:
+                raise ValueError("psf and mult cannot be combined")
+            _check(lib().fir_osem_weighted(self._h, C.byref(proj_desc(proj)), _ptr(sino, n=nb), _ptr(mult, n=nb),
+                                           _ptr(bias, n=nb), C.byref(vol_desc(vol, 1)),
+                                           _ptr(img, writable=True, n=vol.n_voxels),
+                                           _ptr(sens, n=vol.n_voxels * params.n_subsets), C.byref(osem_desc(params)),
+                                           C.cast(cb, C.c_void_p) if cb is not None else None, None))
+            return
         fn = lib().fir_osem_psf if psf else lib().fir_osem
         _check(fn(self._h, C.byref(proj_desc(proj)), _ptr(sino, n=nb), _ptr(bias, n=nb),
                   C.byref(vol_desc(vol, 1)), _ptr(img, writable=True, n=vol.n_voxels),

@@ -602,16 +602,16 @@ void det_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, 
 // widened image + bias) over the subset of s: the fused kernel, or in
 // deterministic mode the ratio kernel followed by the ordered scatter.
 void ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, const double* wimg,
-                       const float* sino, const float* bias, float* bp, long long nvox)
+                       const float* sino, const float* mult, const float* bias, float* bp, long long nvox)
 {
   if (c.backproj == FIR_BACKPROJ_DETERMINISTIC)
   {
     float* ratio = static_cast<float*>(c.ratio.ensure((size_t)std::max(s.n_enum, 1) * sizeof(float)));
-    timed_launch(c, [&] { launch_ratio(g, s, t, wimg, sino, bias, ratio, cfg_of(c)); });
+    timed_launch(c, [&] { launch_ratio(g, s, t, wimg, sino, mult, bias, ratio, cfg_of(c)); });
     det_backproject(c, g, s, t, ratio, true, bp, nvox);
     return;
   }
-  timed_launch(c, [&] { launch_osem_subset(g, s, t, wimg, sino, bias, bp, c.skip_zero != 0, cfg_of(c)); });
+  timed_launch(c, [&] { launch_osem_subset(g, s, t, wimg, sino, mult, bias, bp, c.skip_zero != 0, cfg_of(c)); });
 }
 
 // Double copy of a float image in context scratch, for the projector gathers.
@@ -934,7 +934,7 @@ void check_osem_params(const fir_osem_params* prm, const ProjInfo& p)
 
 // Device-pointer body of one OSEM sub-iteration.
 void osem_subiteration_device(fir_ctx& c, const ProjInfo& p, const Tables& t, const Grid& g,
-                              const VolInfo& v, const float* sino, const float* bias, float* img,
+                              const VolInfo& v, const float* sino, const float* mult, const float* bias, float* img,
                               const float* sens_frame, const fir_osem_params* prm, int subset,
                               int subiter)
 {
@@ -942,7 +942,7 @@ void osem_subiteration_device(fir_ctx& c, const ProjInfo& p, const Tables& t, co
   cuda_ok(cudaMemsetAsync(bp, 0, (size_t)v.nvox * sizeof(float), c.stream), "cudaMemsetAsync");
   const Sino s = sino_of(p, prm->n_subsets, subset);
   const double* wimg = widen(c, img, v.nvox);
-  ratio_backproject(c, g, s, t, wimg, sino, bias, bp, v.nvox);
+  ratio_backproject(c, g, s, t, wimg, sino, mult, bias, bp, v.nvox);
   launch_em_update(v.nvox, img, bp, sens_frame, cfg_of(c));
   after_launch(c);
   const bool conv = prm->convolution_interval > 0 && prm->fwhm_xyz[0] > 0.0 && prm->fwhm_xyz[1] > 0.0 &&
@@ -958,7 +958,7 @@ void osem_subiteration_device(fir_ctx& c, const ProjInfo& p, const Tables& t, co
 // parameters is part of the system model (projection of B x, B applied to
 // the backprojection, sens_frame already blurred).
 void osem_psf_subiteration_device(fir_ctx& c, const ProjInfo& p, const Tables& t, const Grid& g,
-                                  const VolInfo& v, const float* sino, const float* bias, float* img,
+                                  const VolInfo& v, const float* sino, const float* mult, const float* bias, float* img,
                                   const float* sens_frame, const fir_osem_params* prm, int subset, int subiter)
 {
   const size_t bytes = (size_t)v.nvox * sizeof(float);
@@ -969,7 +969,7 @@ void osem_psf_subiteration_device(fir_ctx& c, const ProjInfo& p, const Tables& t
   convolve_device(c, v, blur, prm->fwhm_xyz, prm->cut_radius);
   const Sino s = sino_of(p, prm->n_subsets, subset);
   const double* wimg = widen(c, blur, v.nvox);
-  ratio_backproject(c, g, s, t, wimg, sino, bias, bp, v.nvox);
+  ratio_backproject(c, g, s, t, wimg, sino, mult, bias, bp, v.nvox);
   convolve_device(c, v, bp, prm->fwhm_xyz, prm->cut_radius);
   launch_em_update(v.nvox, img, bp, sens_frame, cfg_of(c));
   after_launch(c);
@@ -983,7 +983,8 @@ void osem_psf_subiteration_device(fir_ctx& c, const ProjInfo& p, const Tables& t
 }
 
 // The OSEM driver of fir_osem and fir_osem_psf (psf: resolution modelling).
-void osem_run(fir_ctx& c, const fir_proj_desc* proj, const float* sino, const float* bias, const fir_vol_desc* vol,
+void osem_run(fir_ctx& c, const fir_proj_desc* proj, const float* sino, const float* mult, const float* bias,
+              const fir_vol_desc* vol,
               float* img, const float* sens, const fir_osem_params* params, fir_osem_save_fn save, void* user,
               bool psf)
 {
@@ -999,6 +1000,7 @@ void osem_run(fir_ctx& c, const fir_proj_desc* proj, const float* sino, const fl
   }
   Stager st(c);
   const float* dsino = st.in(sino, p.g.n_bins);
+  const float* dmult = st.in(mult, p.g.n_bins);
   const float* dbias = st.in(bias, p.g.n_bins);
   const float* dsens = st.in(sens, v.nvox * params->n_subsets);
   float* dimg = st.inout(img, v.nvox);
@@ -1024,11 +1026,11 @@ void osem_run(fir_ctx& c, const fir_proj_desc* proj, const float* sino, const fl
       const float* sframe = dsens + (size_t)subset * v.nvox;
       if (psf)
       {
-        osem_psf_subiteration_device(c, p, t, g, v, dsino, dbias, dimg, sframe, params, subset, subiter);
+        osem_psf_subiteration_device(c, p, t, g, v, dsino, dmult, dbias, dimg, sframe, params, subset, subiter);
       }
       else
       {
-        osem_subiteration_device(c, p, t, g, v, dsino, dbias, dimg, sframe, params, subset, subiter);
+        osem_subiteration_device(c, p, t, g, v, dsino, dmult, dbias, dimg, sframe, params, subset, subiter);
       }
       if (save != nullptr && params->save_interval > 0 && subiter % params->save_interval == 0 &&
           subiter != nsub_total)
@@ -1507,7 +1509,7 @@ fir_status fir_osem_subiteration(fir_ctx* ctx, const fir_proj_desc* proj, const 
     const float* dbias = st.in(bias, p.g.n_bins);
     const float* dsens = st.in(sens_frame, v.nvox);
     float* dimg = st.inout(img, v.nvox);
-    osem_subiteration_device(c, p, t, g, v, dsino, dbias, dimg, dsens, params, subset, subiter);
+    osem_subiteration_device(c, p, t, g, v, dsino, nullptr, dbias, dimg, dsens, params, subset, subiter);
     finish(c, st);
   });
 }
@@ -1516,7 +1518,8 @@ fir_status fir_osem(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, 
                     const fir_vol_desc* vol, float* img, const float* sens, const fir_osem_params* params,
                     fir_osem_save_fn save, void* user)
 {
-  return guarded(__func__, [&] { osem_run(check_ctx(ctx), proj, sino, bias, vol, img, sens, params, save, user, false); });
+  return guarded(__func__, [&] { osem_run(check_ctx(ctx), proj, sino, nullptr, bias, vol, img, sens, params, save, user, false);
+  });
 }
 
 fir_status fir_osem_psf(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const float* bias,
@@ -1527,7 +1530,20 @@ fir_status fir_osem_psf(fir_ctx* ctx, const fir_proj_desc* proj, const float* si
     fir_ctx& c = check_ctx(ctx);
     const bool psf = params != nullptr && params->fwhm_xyz[0] > 0.0f && params->fwhm_xyz[1] > 0.0f &&
                      params->fwhm_xyz[2] > 0.0f;
-    osem_run(c, proj, sino, bias, vol, img, sens, params, save, user, psf);
+    osem_run(c, proj, sino, nullptr, bias, vol, img, sens, params, save, user, psf);
+  });
+}
+
+fir_status fir_osem_weighted(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const float* mult,
+                             const float* bias, const fir_vol_desc* vol, float* img, const float* sens,
+                             const fir_osem_params* params, fir_osem_save_fn save, void* user)
+{
+  return guarded(__func__, [&] {
+    if (mult == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "multiplicative factors must not be NULL");
+    }
+    osem_run(check_ctx(ctx), proj, sino, mult, bias, vol, img, sens, params, save, user, false);
   });
 }
 
@@ -1558,7 +1574,7 @@ fir_status fir_ratio_backprojection(fir_ctx* ctx, const fir_proj_desc* proj, con
     cuda_ok(cudaMemsetAsync(dbp, 0, (size_t)v.nvox * sizeof(float), c.stream), "cudaMemsetAsync");
     const Sino s = sino_of(p, n_subsets, subset);
     const double* wimg = widen(c, dimg, v.nvox);
-    ratio_backproject(c, g, s, t, wimg, dsino, dbias, dbp, v.nvox);
+    ratio_backproject(c, g, s, t, wimg, dsino, nullptr, dbias, dbp, v.nvox);
     finish(c, st);
   });
 }
@@ -2568,7 +2584,7 @@ extern "C" fir_status fir_osem_subiteration_noalloc(const fir_proj_desc* proj, c
     // the accumulator keeps the previous call's sums: clear it
     cuda_ok(cudaMemsetAsync(bp, 0, (size_t)v.nvox * sizeof(float), st), "cudaMemsetAsync");
     launch_widen(v.nvox, img, wide, cfg);
-    launch_osem_subset(g, s, t, wide, sino, bias, bp, false, cfg);
+    launch_osem_subset(g, s, t, wide, sino, nullptr, bias, bp, false, cfg);
     launch_em_update(v.nvox, img, bp, sens_frame, cfg);
     const float* fwhm = params->fwhm_xyz;
     const bool conv = params->convolution_interval > 0 && fwhm[0] > 0.0 && fwhm[1] > 0.0 && fwhm[2] > 0.0;

@@ -118,10 +118,11 @@ __global__ void k_reduce_runs(long long n, const unsigned long long* __restrict_
 
 // The ratio of one OSEM sub-iteration per enumerated LOR
 // (reconAlgos.cc:119-158): measured / (projection + bias) when that exceeds
-// 1e-5, else 0.
+// 1e-5, else 0; with multiplicative factors m, m * measured / (m * projection
+// + bias).
 __global__ void __launch_bounds__(256) k_ratio(Grid g, Sino s, Tables t, const double* __restrict__ img,
-                                               const float* __restrict__ sino, const float* __restrict__ bias,
-                                               float* ratio, int* check)
+                                               const float* __restrict__ sino, const float* __restrict__ mult,
+                                               const float* __restrict__ bias, float* ratio, int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < s.n_enum;
@@ -148,11 +149,21 @@ __global__ void __launch_bounds__(256) k_ratio(Grid g, Sino s, Tables t, const d
   }
   if (valid)
   {
+    const float m = mult != nullptr ? __ldg(mult + l.bin) : 1.0f;
+    if (mult != nullptr)
+    {
+      line = __fmul_rn(line, m);
+    }
     if (bias != nullptr)
     {
       line = __fadd_rn(line, __ldg(bias + l.bin));
     }
-    ratio[i] = (go && ok && (double)line > kEps) ? __fdiv_rn(__ldg(sino + l.bin), line) : 0.0f;
+    float q = (go && ok && (double)line > kEps) ? __fdiv_rn(__ldg(sino + l.bin), line) : 0.0f;
+    if (mult != nullptr)
+    {
+      q = __fmul_rn(q, m);
+    }
+    ratio[i] = q;
   }
 }
 
@@ -173,11 +184,11 @@ unsigned blocks_for(long long n, int block)
 }  // namespace
 
 void launch_ratio(const Grid& g, const Sino& s, const Tables& t, const double* img, const float* sino,
-                  const float* bias, float* ratio, const LaunchCfg& cfg)
+                  const float* mult, const float* bias, float* ratio, const LaunchCfg& cfg)
 {
   if (s.n_enum > 0)
   {
-    k_ratio<<<blocks_for(s.n_enum, cfg.block), cfg.block, 0, cfg.stream>>>(g, s, t, img, sino, bias, ratio,
+    k_ratio<<<blocks_for(s.n_enum, cfg.block), cfg.block, 0, cfg.stream>>>(g, s, t, img, sino, mult, bias, ratio,
                                                                           cfg.check);
   }
 }

@@ -34,8 +34,10 @@ void launch_forward(const Grid& g, const Sino& s, const Tables& t, const double*
                     FwdEpilogue ep, const LaunchCfg& cfg);
 void launch_backward(const Grid& g, const Sino& s, const Tables& t, const float* sino, float* img,
                      bool skip_zero, const LaunchCfg& cfg);
+// mult: per-bin multiplicative factors of the ordinary-Poisson model, or
+// nullptr for FIR's model.
 void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const double* img,
-                        const float* sino, const float* bias, float* bp, bool skip_zero,
+                        const float* sino, const float* mult, const float* bias, float* bp, bool skip_zero,
                         const LaunchCfg& cfg);
 void launch_siddon_paths(const Grid& g, long long n, const double* ends, int cap, int* coords,
                          double* lengths, int* counts, int* crosses, const LaunchCfg& cfg);
@@ -45,8 +47,9 @@ void launch_lor_paths(const Grid& g, const Sino& s, const Tables& t, long long n
 
 // deterministic.cu
 // ratio[i] = sino / (projection + bias) for enumerated LOR i, or 0
+// (with mult: m * sino / (m * projection + bias))
 void launch_ratio(const Grid& g, const Sino& s, const Tables& t, const double* img, const float* sino,
-                  const float* bias, float* ratio, const LaunchCfg& cfg);
+                  const float* mult, const float* bias, float* ratio, const LaunchCfg& cfg);
 // Device scratch of at least `bytes` for slot 0 (per-LOR counts and
 // offsets) or slot 1 (pairs and sort space); nullptr if unavailable.
 using ScratchFn = std::function<void*(int slot, size_t bytes)>;

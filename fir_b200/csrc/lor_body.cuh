@@ -22,10 +22,15 @@ __device__ __forceinline__ void flag(int* check, int bit)
 // identical voxels with identical lengths.  Every lane of the warp must call
 // this (lanes with i >= n_enum are idle), since it re-converges the warp
 // between the traversals.
-__device__ __forceinline__ void osem_lor(const Grid& g, const Sino& s, int subset, const Tables& t,
-                                         const double* __restrict__ img, const float* __restrict__ sino,
-                                         const float* __restrict__ bias, float* bp, bool skip_zero, int i,
-                                         int* check)
+//
+// kWeighted: the ordinary-Poisson model with multiplicative factors m
+// (attenuation, normalisation) per bin: estimate m * line + bias, and the
+// backprojected value m * measured / estimate.  Without it the body is FIR's.
+template<bool kWeighted>
+__device__ __forceinline__ void osem_lor_body(const Grid& g, const Sino& s, int subset, const Tables& t,
+                                              const double* __restrict__ img, const float* __restrict__ sino,
+                                              const float* __restrict__ mult, const float* __restrict__ bias,
+                                              float* bp, bool skip_zero, int i, int* check)
 {
   // bp may come from a descriptor in memory, not a kernel parameter: without
   // this the compiler cannot tell the atomic's address space and tests it at
@@ -57,12 +62,22 @@ __device__ __forceinline__ void osem_lor(const Grid& g, const Sino& s, int subse
     }
   });
   __syncwarp();
+  const float m = kWeighted && valid ? __ldg(mult + l.bin) : 1.0f;
+  if (kWeighted)
+  {
+    line = __fmul_rn(line, m);
+  }
   if (valid && bias != nullptr)
   {
     line = __fadd_rn(line, __ldg(bias + l.bin));
   }
   const bool back = go && ok && (double)line > kEps;
-  const double ratio = back ? (double)__fdiv_rn(y, line) : 0.0;
+  float q = back ? __fdiv_rn(y, line) : 0.0f;
+  if (kWeighted)
+  {
+    q = __fmul_rn(q, m);
+  }
+  const double ratio = (double)q;
   ok = siddon_walk(g, w, back, [&](bool inside, int c, double len) {
          if (inside)
          {
@@ -73,5 +88,13 @@ __device__ __forceinline__ void osem_lor(const Grid& g, const Sino& s, int subse
   {
     flag(check, kCheckWalkGuard);
   }
+}
+// FIR's sub-iteration body (reconAlgos.cc:119-158).
+__device__ __forceinline__ void osem_lor(const Grid& g, const Sino& s, int subset, const Tables& t,
+                                         const double* __restrict__ img, const float* __restrict__ sino,
+                                         const float* __restrict__ bias, float* bp, bool skip_zero, int i,
+                                         int* check)
+{
+  osem_lor_body<false>(g, s, subset, t, img, sino, nullptr, bias, bp, skip_zero, i, check);
 }
 }  // namespace fir

@@ -98,15 +98,17 @@ __global__ void __launch_bounds__(256) k_backward(Grid g, Sino s, Tables t,
 }
 
 // One OSEM sub-iteration over the subset of s: one thread per enumerated
-// LOR (reconAlgos.cc:119-158).
+// LOR (reconAlgos.cc:119-158); kWeighted adds the multiplicative factors.
+template<bool kWeighted>
 __global__ void __launch_bounds__(256, 4) k_osem_subset(Grid g, Sino s, Tables t,
-                                                     const double* __restrict__ img,
-                                                     const float* __restrict__ sino,
-                                                     const float* __restrict__ bias, float* bp,
-                                                     int skip_zero, int* check)
+                                                        const double* __restrict__ img,
+                                                        const float* __restrict__ sino,
+                                                        const float* __restrict__ mult,
+                                                        const float* __restrict__ bias, float* bp,
+                                                        int skip_zero, int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  osem_lor(g, s, s.subset, t, img, sino, bias, bp, skip_zero != 0, i, check);
+  osem_lor_body<kWeighted>(g, s, s.subset, t, img, sino, mult, bias, bp, skip_zero != 0, i, check);
 }
 
 // Path dump of one segment into row i of coords / lengths.
@@ -218,15 +220,24 @@ void launch_backward(const Grid& g, const Sino& s, const Tables& t, const float*
 }
 
 void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const double* img,
-                        const float* sino, const float* bias, float* bp, bool skip_zero,
+                        const float* sino, const float* mult, const float* bias, float* bp, bool skip_zero,
                         const LaunchCfg& cfg)
 {
   if (s.n_enum == 0)
   {
     return;
   }
-  k_osem_subset<<<blocks_for(s.n_enum, cfg.block), cfg.block, 0, cfg.stream>>>(
-    g, s, t, img, sino, bias, bp, skip_zero ? 1 : 0, cfg.check);
+  const unsigned nb = blocks_for(s.n_enum, cfg.block);
+  if (mult != nullptr)
+  {
+    k_osem_subset<true><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, sino, mult, bias, bp, skip_zero ? 1 : 0,
+                                                          cfg.check);
+  }
+  else
+  {
+    k_osem_subset<false><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, sino, nullptr, bias, bp, skip_zero ? 1 : 0,
+                                                           cfg.check);
+  }
 }
 
 void launch_siddon_paths(const Grid& g, long long n, const double* ends, int cap, int* coords,

@@ -289,6 +289,19 @@ fir_status fir_osem_psf(fir_ctx* ctx, const fir_proj_desc* proj, const float* si
                         const fir_vol_desc* vol, float* img, const float* sens, const fir_osem_params* params,
                         fir_osem_save_fn save, void* user);
 
+/* OSEM with the ordinary-Poisson system model: the mean of bin i is
+ * m_i (A x)_i + bias_i, with m the per-bin multiplicative factors
+ * (attenuation exp(-A mu) = 1 / ACF, normalisation), instead of FIR's
+ * precorrected data with mean (A x)_i + bias_i (reconAlgos.cc:119-158,
+ * OSEM.cc:314-338).  Each bin backprojects m_i y_i / (m_i (A x)_i + bias_i)
+ * when the denominator exceeds 1e-5.  sino holds the measured counts (not
+ * precorrected); sens holds the n_subsets frames A_s^T m (fir_backward of
+ * mult).  Float arithmetic: line * m, + bias, y / estimate, * m.  With m = 1
+ * this is fir_osem.  No counterpart in FIR, which only precorrects. */
+fir_status fir_osem_weighted(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const float* mult,
+                             const float* bias, const fir_vol_desc* vol, float* img, const float* sens,
+                             const fir_osem_params* params, fir_osem_save_fn save, void* user);
+
 /* ---- multi-frame projection ----
  *
  * Element type of the multi-frame projectors' data. */

@@ -135,6 +135,8 @@ class Restated:
         L.fo_osem.argtypes = [C.POINTER(FoProj), _f32p, C.c_void_p, C.POINTER(FoVol), C.c_int, _f64p, _f64p,
                               _f32p, _f32p, C.POINTER(FoOsem)]
         L.fo_osem_psf.argtypes = L.fo_osem.argtypes
+        L.fo_osem_weighted.argtypes = [C.POINTER(FoProj), _f32p, _f32p, C.c_void_p, C.POINTER(FoVol), C.c_int,
+                                       _f64p, _f64p, _f32p, _f32p, C.POINTER(FoOsem)]
         L.fo_bin_coordinates.argtypes = [C.POINTER(FoProj)] + [C.c_int] * 4 + [C.POINTER(C.c_int)] * 4
         L.fo_rebin_weight.argtypes = [C.POINTER(FoProj), _f32p]
         L.fo_em_update.argtypes = [C.c_longlong, _f32p, _f32p, _f32p]
@@ -237,8 +239,10 @@ class Restated:
     def sensitivity(self, s, p, v, n_subsets: int = 1, truncate: bool = True):
         return self.backward(s, p, v, None, n_subsets, truncate)
 
-    def osem(self, s, p, v, sino, img, sens, prm: OSEMParams, bias=None, truncate: bool = True, psf: bool = False):
-        """reconAlgos::OSEM; with psf, the corrected resolution-modelling OSEM."""
+    def osem(self, s, p, v, sino, img, sens, prm: OSEMParams, bias=None, truncate: bool = True, psf: bool = False,
+             mult=None):
+        """reconAlgos::OSEM; with psf, the corrected resolution-modelling OSEM;
+        with mult, the ordinary-Poisson model with multiplicative factors."""
         f = self.proj(p)
         xy, z = self.scanner_tables(s)
         img = np.ascontiguousarray(img, np.float32).copy().ravel()
@@ -246,6 +250,11 @@ class Restated:
         o.fwhm[:] = [float(x) for x in prm.fwhm_xyz]
         bias_arr = None if bias is None else np.ascontiguousarray(bias, np.float32)
         bptr = None if bias_arr is None else bias_arr.ctypes.data_as(C.c_void_p)
+        if mult is not None:
+            self.L.fo_osem_weighted(C.byref(f), np.ascontiguousarray(sino, np.float32),
+                                    np.ascontiguousarray(mult, np.float32), bptr, C.byref(fo_vol(v)), int(truncate),
+                                    xy, z, img, np.ascontiguousarray(sens, np.float32).ravel(), C.byref(o))
+            return img.reshape(v.shape_zyx)
         fn = self.L.fo_osem_psf if psf else self.L.fo_osem
         fn(C.byref(f), np.ascontiguousarray(sino, np.float32), bptr, C.byref(fo_vol(v)), int(truncate), xy, z, img,
            np.ascontiguousarray(sens, np.float32).ravel(), C.byref(o))

@@ -608,16 +608,18 @@ void fo_proj_multiply(long long n, float* a, const float* b)
 }
 
 /* ---- OSEM: reconAlgos.cc:11-59 (getLine), :63-201 (loop) ---- */
-/* The OSEM loop of reconAlgos.cc:63-201.  With psf, the resolution-modelling
+/* The OSEM loop of reconAlgos.cc:63-201.  With mult (per-bin multiplicative
+ * factors), the ordinary-Poisson model: estimate m * line + bias, and the
+ * backprojected value m * measured / estimate.  With psf, the resolution-modelling
  * variant that OSEM_ResoReco (reconAlgos.cc:203-367) intends, corrected: the
  * Gaussian B = operations::convolve(fwhm, cutRadius) sits inside the system
  * model.  Each sub-iteration projects B x (FIR projects x, :296), blurs the
  * backprojection (:300-304), and divides it by the blurred sensitivity of
  * the subset before the usual EM update (FIR divides the image, :323);
  * every sensitivity frame is blurred once before the loop. */
-static void osem_loop(const fo_proj* p, const float* sino, const float* bias, const fo_vol* v, int truncate,
-                      const double* xy, const double* z, float* img, const float* sens, const fo_osem_params* prm,
-                      int psf)
+static void osem_loop(const fo_proj* p, const float* sino, const float* mult, const float* bias, const fo_vol* v,
+                      int truncate, const double* xy, const double* z, float* img, const float* sens,
+                      const fo_osem_params* prm, int psf)
 {
   fo_grid g;
   fo_grid_init(&g, v, truncate);
@@ -669,10 +671,12 @@ static void osem_loop(const fo_proj* p, const float* sino, const float* bias, co
               float line = 0.0f;
               if (crosses)
                 for (int k = 0; k < n; ++k) line = (float)((double)line + le[k] * (double)model[co[k]]);
+              if (mult) line = line * mult[bin];
               if (bias) line += bias[bin];
               if ((double)line > FO_EPS)
               {
-                const float ratio = sino[bin] / line;
+                float ratio = sino[bin] / line;
+                if (mult) ratio = ratio * mult[bin];
                 for (int k = 0; k < n; ++k) bp[co[k]] = (float)((double)bp[co[k]] + le[k] * (double)ratio);
               }
             }
@@ -694,14 +698,21 @@ static void osem_loop(const fo_proj* p, const float* sino, const float* bias, co
 void fo_osem(const fo_proj* p, const float* sino, const float* bias, const fo_vol* v, int truncate,
              const double* xy, const double* z, float* img, const float* sens, const fo_osem_params* prm)
 {
-  osem_loop(p, sino, bias, v, truncate, xy, z, img, sens, prm, 0);
+  osem_loop(p, sino, NULL, bias, v, truncate, xy, z, img, sens, prm, 0);
+}
+
+void fo_osem_weighted(const fo_proj* p, const float* sino, const float* mult, const float* bias, const fo_vol* v,
+                      int truncate, const double* xy, const double* z, float* img, const float* sens,
+                      const fo_osem_params* prm)
+{
+  osem_loop(p, sino, mult, bias, v, truncate, xy, z, img, sens, prm, 0);
 }
 
 void fo_osem_psf(const fo_proj* p, const float* sino, const float* bias, const fo_vol* v, int truncate,
                  const double* xy, const double* z, float* img, const float* sens, const fo_osem_params* prm)
 {
   const int psf = prm->fwhm[0] > 0.0 && prm->fwhm[1] > 0.0 && prm->fwhm[2] > 0.0;
-  osem_loop(p, sino, bias, v, truncate, xy, z, img, sens, prm, psf);
+  osem_loop(p, sino, NULL, bias, v, truncate, xy, z, img, sens, prm, psf);
 }
 
 /* ProjData::getBinCoordinates (ProjData.cc:342-479): the sinogram bin of the

@@ -106,6 +106,12 @@ void fo_osem_psf(const fo_proj* p, const float* sino, const float* bias, const f
 
 void fo_em_update(long long n, float* img, float* bp, const float* sens);
 
+/* OSEM with per-bin multiplicative factors m (ordinary-Poisson model):
+ * estimate m * (A x) + bias; the backprojected value is m * y / estimate. */
+void fo_osem_weighted(const fo_proj* p, const float* sino, const float* mult, const float* bias,
+                      const fo_vol* v, int truncate, const double* xy, const double* z, float* img,
+                      const float* sens, const fo_osem_params* prm);
+
 /* ProjData::getBinCoordinates: 1 and the bin of the crystal pair, or 0. */
 int fo_bin_coordinates(const fo_proj* p, int r1, int c1, int r2, int c2, int* seg, int* view, int* axial,
                        int* tang);

@@ -442,3 +442,37 @@ def test_rebin_weight_matches_oracle(gpu_ctx_factory, restated, torch, k):
     ctx.proj_rebin_weight(p, dev)
     torch.cuda.synchronize()
     np.testing.assert_array_equal(dev.cpu().numpy(), want)
+
+
+# ------------------------------------------- ordinary-Poisson (weighted) OSEM
+
+def test_osem_weighted_matches_oracle(gpu_ctx_factory, restated):
+    """fir_osem_weighted: measured counts with attenuation factors m = 1 / ACF
+    in the model and A_s^T m as sensitivity.  Atomic mode within 1e-4 of the
+    restatement, deterministic mode bit-identical to it, and m = 1 gives
+    fir_osem."""
+    w = workloads.small()
+    x = workloads.activity(w)
+    mu = restated.hu_to_mu(workloads.hounsfield(w))
+    acf = restated.exponential(restated.forward(w.scanner, w.proj, w.vol, mu))
+    m = (1.0 / acf).astype(np.float32)
+    expect = (restated.forward(w.scanner, w.proj, w.vol, x) * m).astype(np.float32)
+    y = workloads.poisson_counts(expect, w.counts, 11)
+    sens = restated.backward(w.scanner, w.proj, w.vol.with_frames(4), m, 4)
+    bias = np.full(w.n_lors, 0.01, np.float32)
+    prm = OSEMParams(n_iterations=2, n_subsets=4, convolution_interval=1, fwhm_xyz=[4.0, 4.0, 4.0],
+                     cut_radius=115.0)
+    want = restated.osem(w.scanner, w.proj, w.vol, y, np.ones_like(x), sens, prm, bias=bias, mult=m)
+    got = np.ones_like(x)
+    gpu_ctx_factory(w.scanner).osem(w.proj, y, w.vol, got, sens, prm, bias=bias, mult=m)
+    assert rel_l2(got, want) <= 1e-4
+    det = gpu_ctx_factory(w.scanner)
+    det.set_option(capi.FIR_OPT_BACKPROJ_MODE, capi.FIR_BACKPROJ_DETERMINISTIC)
+    got_det = np.ones_like(x)
+    det.osem(w.proj, y, w.vol, got_det, sens, prm, bias=bias, mult=m)
+    np.testing.assert_array_equal(got_det, want)
+    ones = np.ones_like(m)
+    a, b = np.ones_like(x), np.ones_like(x)
+    det.osem(w.proj, y, w.vol, a, sens, prm, mult=ones)
+    det.osem(w.proj, y, w.vol, b, sens, prm)
+    np.testing.assert_array_equal(a, b)

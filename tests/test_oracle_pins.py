@@ -301,3 +301,19 @@ def test_rebin_weight_multi_segment_by_counting(restated, k):
         base += f.n_views * nax * f.n_tang_coords
     np.testing.assert_array_equal(got, want)
     assert (got < 1).any()
+
+
+def test_oracle_weighted_osem_with_unit_factors_is_osem(restated):
+    """The ordinary-Poisson OSEM of the restatement with m = 1 is
+    bit-identical to its OSEM."""
+    from fir_b200 import workloads
+    from fir_b200.geometry import OSEMParams
+
+    w = workloads.tiny()
+    x = workloads.activity(w)
+    y = workloads.poisson_counts(restated.forward(w.scanner, w.proj, w.vol, x), w.counts, 1)
+    sens = restated.sensitivity(w.scanner, w.proj, w.vol, 4)
+    prm = OSEMParams(n_iterations=2, n_subsets=4, convolution_interval=1, fwhm_xyz=[4.0, 4.0, 4.0])
+    a = restated.osem(w.scanner, w.proj, w.vol, y, np.ones_like(x), sens, prm)
+    b = restated.osem(w.scanner, w.proj, w.vol, y, np.ones_like(x), sens, prm, mult=np.ones_like(y))
+    np.testing.assert_array_equal(a, b)
