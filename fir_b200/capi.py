@@ -25,6 +25,7 @@ FIR_OPT_SKIP_ZERO_BINS = 3
 FIR_OPT_BLOCK_SIZE = 4
 FIR_OPT_TIMING = 5
 FIR_OPT_DETERMINISTIC_CHUNK = 6
+FIR_OPT_STEP_LIMIT = 7
 FIR_GEOMETRY_REFERENCE = 0
 FIR_GEOMETRY_EXACT = 1
 FIR_BACKPROJ_ATOMIC = 0

@@ -485,6 +485,7 @@ struct fir_ctx
   int skip_zero = 0;
   int block = 128;
   long long det_chunk = 1LL << 28;
+  int step_limit = 0;  // FIR_OPT_STEP_LIMIT
   long long launches = 0;
 
   bool have_scanner = false;
@@ -683,6 +684,12 @@ Grid grid_of(const fir_ctx& c, const VolInfo& v)
     fail(FIR_ERR_NOT_SUPPORTED, "volume spans ", bound, " traversal steps");
   }
   g.guard = (int)bound;
+  g.exact_only = 0;
+  if (c.step_limit > 0)
+  {
+    g.guard = std::min(g.guard, c.step_limit);
+    g.exact_only = 1;
+  }
   return g;
 }
 
@@ -1221,6 +1228,13 @@ fir_status fir_ctx_set_option(fir_ctx* ctx, fir_option opt, int value)
     case FIR_OPT_TIMING:
       c.timing = value != 0;
       break;
+    case FIR_OPT_STEP_LIMIT:
+      if (value < 0)
+      {
+        fail(FIR_ERR_INVALID_ARGUMENT, "step limit must not be negative");
+      }
+      c.step_limit = value;
+      break;
     case FIR_OPT_DETERMINISTIC_CHUNK:
       if (value < 0)
       {
@@ -1272,6 +1286,7 @@ fir_status fir_ctx_get_option(fir_ctx* ctx, fir_option opt, int* value)
     case FIR_OPT_BLOCK_SIZE: *value = c.block; break;
     case FIR_OPT_TIMING: *value = c.timing ? 1 : 0; break;
     case FIR_OPT_DETERMINISTIC_CHUNK: *value = (int)std::min<long long>(c.det_chunk, 0x7fffffff); break;
+    case FIR_OPT_STEP_LIMIT: *value = c.step_limit; break;
     default: fail(FIR_ERR_INVALID_ARGUMENT, "unknown option ", (int)opt);
     }
   });

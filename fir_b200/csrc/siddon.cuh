@@ -25,6 +25,7 @@ struct Grid
 {
   int nx, ny, nz, nxy;
   int guard;       // bound on traversal steps: planes crossed in all dimensions + margin
+  int exact_only;  // 1: always FIR's subtraction tie test, bounded by guard (testing aid)
   double ext[3];   // step sizes: FIR's int-truncated extents, or the real ones
   double low[3];   // border planes: x,y = offset - voxel/2, z = offset - depth/2
   double high[3];  // low + n * voxel (real voxel extents, as in FIR)
@@ -434,7 +435,8 @@ __device__ __forceinline__ bool siddon_walk(const Grid& g, Walk w, bool go, Emit
   const bool active = go && prev < w.amax;
   // every alpha of the walk is >= the smallest initial one (alphas only
   // grow, alphaMax > alphaMin), so this decides the tie form for the walk
-  const bool fast = !active || min_of(w.amin, min_of(w.a[0], min_of(w.a[1], w.a[2]))) >= kEps;
+  const bool fast =
+    !active || (!g.exact_only && min_of(w.amin, min_of(w.a[0], min_of(w.a[1], w.a[2]))) >= kEps);
   if (__all_sync(__activemask(), fast))
   {
     walk_loop_fast(w, prev, active, emit);

@@ -149,7 +149,14 @@ typedef enum fir_option
   /* Deterministic backprojection works on chunks of at most this many
    * (voxel, contribution) pairs (16 bytes each, twice, plus sort space);
    * 0 restores the default of 2^28.  Any chunk size gives the same result. */
-  FIR_OPT_DETERMINISTIC_CHUNK = 6
+  FIR_OPT_DETERMINISTIC_CHUNK = 6,
+  /* Testing aid for failure reporting.  k > 0 bounds every traversal at k
+   * steps and evaluates FIR's tie test as written (no fast form); a traversal
+   * that reaches the bound before its end sets the device check word, and
+   * the call reports FIR_ERR_DEVICE_CHECK (host buffers) or the next
+   * fir_ctx_synchronize does.  Results past the bound are truncated.  0
+   * (default): the natural bound, which only non-finite input can reach. */
+  FIR_OPT_STEP_LIMIT = 7
 } fir_option;
 
 enum

@@ -476,3 +476,37 @@ def test_osem_weighted_matches_oracle(gpu_ctx_factory, restated):
     det.osem(w.proj, y, w.vol, a, sens, prm, mult=ones)
     det.osem(w.proj, y, w.vol, b, sens, prm)
     np.testing.assert_array_equal(a, b)
+
+
+# ------------------------------------------- failure reporting
+
+def test_step_bound_is_reported_and_the_context_recovers(gpu_ctx_factory, restated, torch):
+    """A traversal that reaches its step bound sets the device check word; the
+    call reports FIR_ERR_DEVICE_CHECK (host buffers at once, device buffers at
+    the next synchronize) and the context stays usable.  The bound is forced
+    with FIR_OPT_STEP_LIMIT, so no GPU fault is involved.  A bound that no
+    path reaches gives FIR's projection bit for bit, which also checks the
+    exact tie test against the fast one on every LOR of the workload."""
+    w = workloads.small()
+    ctx = gpu_ctx_factory(w.scanner)
+    x = workloads.activity(w)
+    want = restated.forward(w.scanner, w.proj, w.vol, x)
+    out = np.zeros(w.n_lors, np.float32)
+    ctx.set_option(capi.FIR_OPT_STEP_LIMIT, 3)
+    assert ctx.get_option(capi.FIR_OPT_STEP_LIMIT) == 3
+    with pytest.raises(capi.FirError, match="iteration bound") as e:
+        ctx.forward(w.vol, x, w.proj, out)
+    assert e.value.status == 4  # FIR_ERR_DEVICE_CHECK
+    dx = torch.from_numpy(x).cuda()
+    dout = torch.empty(w.n_lors, device="cuda")
+    ctx.forward(w.vol, dx, w.proj, dout)  # enqueued; reported at the synchronize
+    with pytest.raises(capi.FirError, match="iteration bound"):
+        ctx.synchronize()
+    ctx.set_option(capi.FIR_OPT_STEP_LIMIT, 1_000_000)
+    ctx.forward(w.vol, x, w.proj, out)
+    np.testing.assert_array_equal(out, want)
+    ctx.set_option(capi.FIR_OPT_STEP_LIMIT, 0)
+    ctx.forward(w.vol, x, w.proj, out)
+    np.testing.assert_array_equal(out, want)
+    with pytest.raises(capi.FirError, match="must not be negative"):
+        ctx.set_option(capi.FIR_OPT_STEP_LIMIT, -1)
