@@ -498,6 +498,11 @@ struct fir_ctx
   DevBuf bp, conv1, conv2, conv_copy, mu, wide, det, det_pairs, ratio, frames_il, frames_acc, psf_blur, psf_sens, rebin;
   std::vector<DevBuf> staging;
 
+  // pipelined input of fir_osem from pinned host memory
+  std::vector<DevBuf> pipe;
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> pipe_events;
+
   // projector-kernel timing (FIR_OPT_TIMING)
   bool timing = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -720,6 +725,23 @@ Sino sino_of(const ProjInfo& p, int n_subsets, int subset)
   s.enum_base[s.n_segments] = (int)(base / n_subsets);
   s.n_enum = (int)(base / n_subsets);
   return s;
+}
+
+// Page-locked host memory (cudaHostAlloc / cudaHostRegister), which the copy
+// engines read asynchronously.
+bool is_pinned_host(const void* p)
+{
+  if (p == nullptr)
+  {
+    return false;
+  }
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess)
+  {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
 }
 
 bool is_device_ptr(const void* p)
@@ -989,6 +1011,90 @@ void osem_psf_subiteration_device(fir_ctx& c, const ProjInfo& p, const Tables& t
   cut_device(c, v, img, prm->cut_radius, 1);
 }
 
+// Input of an OSEM run copied subset by subset from pinned host memory, on a
+// copy stream of the context, so that sub-iteration s of the first iteration
+// waits only for its own bins and sensitivity frame: the copies of the next
+// subsets overlap the computation.  Subset s holds views v with
+// v % n_subsets == s (LORCache.cc:49-51), so in every segment its bins are
+// view blocks at a fixed stride: one 2-D copy per segment and array.
+class SubsetFeed
+{
+public:
+  SubsetFeed(fir_ctx& c, const ProjInfo& p, long long nvox, int n_subsets): c_(c), p_(p), nvox_(nvox), nsub_(n_subsets)
+  {
+    if (c.copy_stream == nullptr)
+    {
+      cuda_ok(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    }
+    while ((int)c.pipe_events.size() < n_subsets + 1)
+    {
+      cudaEvent_t e;
+      cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+      c.pipe_events.push_back(e);
+    }
+    if (c.pipe.size() < 4)
+    {
+      c.pipe.resize(4);
+    }
+    // the previous call's kernels may still read the buffers
+    cuda_ok(cudaEventRecord(c.pipe_events[n_subsets], c.stream), "cudaEventRecord");
+    cuda_ok(cudaStreamWaitEvent(c.copy_stream, c.pipe_events[n_subsets], 0), "cudaStreamWaitEvent");
+  }
+
+  // Device buffer (slot 0..2) for a per-bin host array, or nullptr.
+  const float* bins(int slot, const float* host)
+  {
+    if (host == nullptr)
+    {
+      return nullptr;
+    }
+    auto* d = static_cast<float*>(c_.pipe[(size_t)slot].ensure((size_t)p_.g.n_bins * sizeof(float)));
+    arrays_.push_back({host, d});
+    return d;
+  }
+
+  const float* frames(const float* host)
+  {
+    sens_host_ = host;
+    sens_dev_ = static_cast<float*>(c_.pipe[3].ensure((size_t)nvox_ * nsub_ * sizeof(float)));
+    return sens_dev_;
+  }
+
+  // Copies subset s and makes the context's stream wait for it.
+  void feed(int s)
+  {
+    const int vps = p_.g.n_views / nsub_;
+    size_t base = 0;
+    for (int k = 0; k < p_.d.n_segments; ++k)
+    {
+      const size_t bpv = (size_t)p_.n_axial[(size_t)k] * p_.g.n_tang_coords;
+      const size_t off = base + (size_t)s * bpv;
+      const size_t pitch = (size_t)nsub_ * bpv * sizeof(float);
+      for (const auto& a : arrays_)
+      {
+        cuda_ok(cudaMemcpy2DAsync(a.second + off, pitch, a.first + off, pitch, bpv * sizeof(float), (size_t)vps,
+                                  cudaMemcpyHostToDevice, c_.copy_stream),
+                "cudaMemcpy2DAsync");
+      }
+      base += bpv * (size_t)p_.g.n_views;
+    }
+    cuda_ok(cudaMemcpyAsync(sens_dev_ + (size_t)s * nvox_, sens_host_ + (size_t)s * nvox_,
+                            (size_t)nvox_ * sizeof(float), cudaMemcpyHostToDevice, c_.copy_stream),
+            "cudaMemcpyAsync");
+    cuda_ok(cudaEventRecord(c_.pipe_events[(size_t)s], c_.copy_stream), "cudaEventRecord");
+    cuda_ok(cudaStreamWaitEvent(c_.stream, c_.pipe_events[(size_t)s], 0), "cudaStreamWaitEvent");
+  }
+
+private:
+  fir_ctx& c_;
+  const ProjInfo& p_;
+  long long nvox_;
+  int nsub_;
+  std::vector<std::pair<const float*, float*>> arrays_;
+  const float* sens_host_ = nullptr;
+  float* sens_dev_ = nullptr;
+};
+
 // The OSEM driver of fir_osem and fir_osem_psf (psf: resolution modelling).
 void osem_run(fir_ctx& c, const fir_proj_desc* proj, const float* sino, const float* mult, const float* bias,
               const fir_vol_desc* vol,
@@ -1005,11 +1111,28 @@ void osem_run(fir_ctx& c, const fir_proj_desc* proj, const float* sino, const fl
   {
     fail(FIR_ERR_INVALID_ARGUMENT, "sinogram, image and sensitivity must not be NULL");
   }
+  // pinned host inputs stream in subset by subset (the blurred sensitivity
+  // of the PSF model needs all frames at once, so it is staged whole)
+  const bool pipelined = !psf && is_pinned_host(sino) && is_pinned_host(sens) &&
+                         (mult == nullptr || is_pinned_host(mult)) && (bias == nullptr || is_pinned_host(bias));
   Stager st(c);
-  const float* dsino = st.in(sino, p.g.n_bins);
-  const float* dmult = st.in(mult, p.g.n_bins);
-  const float* dbias = st.in(bias, p.g.n_bins);
-  const float* dsens = st.in(sens, v.nvox * params->n_subsets);
+  std::unique_ptr<SubsetFeed> feed;
+  const float *dsino, *dmult, *dbias, *dsens;
+  if (pipelined)
+  {
+    feed = std::make_unique<SubsetFeed>(c, p, v.nvox, params->n_subsets);
+    dsino = feed->bins(0, sino);
+    dmult = feed->bins(1, mult);
+    dbias = feed->bins(2, bias);
+    dsens = feed->frames(sens);
+  }
+  else
+  {
+    dsino = st.in(sino, p.g.n_bins);
+    dmult = st.in(mult, p.g.n_bins);
+    dbias = st.in(bias, p.g.n_bins);
+    dsens = st.in(sens, v.nvox * params->n_subsets);
+  }
   float* dimg = st.inout(img, v.nvox);
   if (psf)
   {
@@ -1031,6 +1154,10 @@ void osem_run(fir_ctx& c, const fir_proj_desc* proj, const float* sino, const fl
     {
       const int subiter = iter * params->n_subsets + subset + 1;
       const float* sframe = dsens + (size_t)subset * v.nvox;
+      if (feed && iter == 0)
+      {
+        feed->feed(subset);
+      }
       if (psf)
       {
         osem_psf_subiteration_device(c, p, t, g, v, dsino, dmult, dbias, dimg, sframe, params, subset, subiter);
@@ -1168,6 +1295,19 @@ fir_status fir_ctx_destroy(fir_ctx* c)
     for (auto& b : c->staging)
     {
       b.release();
+    }
+    if (c->copy_stream != nullptr)
+    {
+      cudaStreamSynchronize(c->copy_stream);
+      cudaStreamDestroy(c->copy_stream);
+    }
+    for (auto& b : c->pipe)
+    {
+      b.release();
+    }
+    for (auto e : c->pipe_events)
+    {
+      cudaEventDestroy(e);
     }
     for (auto& p : c->ev_pending)
     {
