@@ -3,13 +3,14 @@
 // FIR adds every contribution to its voxel as voxel = float(double(voxel) +
 // length * value) (VolData.cc:373-385).  With float atomics the result
 // depends on the order in which LORs reach a voxel.  Here every contribution
-// becomes a (key, product) pair: the key is the voxel index in the high bits
-// and the LOR's enumeration index in the low bits.  The enumeration index is
-// FIR's serial loop order (subset, segment, view of the subset, axial plane,
-// tangential bin; LORCache.cc:10-81).  After a radix sort on the key, each
-// voxel's run holds its contributions in that order, and one thread per run
-// accumulates them with FIR's rounding.  The result equals a single-threaded
-// FIR run bit for bit, and is independent of scheduling.
+// becomes a (voxel, product) pair, written at an offset that follows FIR's
+// serial loop order: LORs in enumeration order (subset, segment, view of the
+// subset, axial plane, tangential bin; LORCache.cc:10-81), then path order.
+// A path visits a voxel at most once.  A stable radix sort on the voxel
+// index alone (32-bit keys, only the bits the volume needs) therefore leaves
+// each voxel's run in FIR's LOR order, and one thread per run accumulates it
+// with FIR's rounding.  The result equals a single-threaded FIR run bit for
+// bit, and is independent of scheduling.
 //
 // Work is chunked over contiguous ranges of LORs; chunks are reduced in
 // order, each run continuing from the voxel's value after the previous
@@ -62,7 +63,7 @@ __global__ void __launch_bounds__(256) k_count(Grid g, Sino s, Tables t, const f
 __global__ void __launch_bounds__(256) k_emit(Grid g, Sino s, Tables t, const float* __restrict__ vals,
                                               int vals_by_enum, int first, int last,
                                               const long long* __restrict__ offsets, long long base,
-                                              int enum_bits, unsigned long long* keys, double* prods)
+                                              unsigned* keys, double* prods)
 {
   const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < last;
@@ -83,11 +84,10 @@ __global__ void __launch_bounds__(256) k_emit(Grid g, Sino s, Tables t, const fl
       go = siddon_setup(g, e, w);
     }
   }
-  const unsigned long long lor = (unsigned long long)i;
   siddon_walk(g, w, go, [&](bool inside, int c, double len) {
     if (inside)
     {
-      keys[at] = ((unsigned long long)c << enum_bits) | lor;
+      keys[at] = (unsigned)c;
       prods[at] = dmul(len, v);
       ++at;
     }
@@ -95,21 +95,21 @@ __global__ void __launch_bounds__(256) k_emit(Grid g, Sino s, Tables t, const fl
 }
 
 // One thread per run of equal voxel: FIR's sequential accumulation.
-__global__ void k_reduce_runs(long long n, const unsigned long long* __restrict__ keys,
-                              const double* __restrict__ prods, int enum_bits, float* img)
+__global__ void k_reduce_runs(long long n, const unsigned* __restrict__ keys, const double* __restrict__ prods,
+                              float* img)
 {
   const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (j >= n)
   {
     return;
   }
-  const unsigned long long voxel = keys[j] >> enum_bits;
-  if (j > 0 && (keys[j - 1] >> enum_bits) == voxel)
+  const unsigned voxel = keys[j];
+  if (j > 0 && keys[j - 1] == voxel)
   {
     return;
   }
   float acc = img[voxel];
-  for (long long k = j; k < n && (keys[k] >> enum_bits) == voxel; ++k)
+  for (long long k = j; k < n && keys[k] == voxel; ++k)
   {
     acc = __double2float_rn(dadd((double)acc, prods[k]));
   }
@@ -261,28 +261,27 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
     max_pairs = g.guard;
   }
   size_t sort_bytes = 0;
-  e = cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const unsigned long long*)nullptr,
-                                      (unsigned long long*)nullptr, (const double*)nullptr, (double*)nullptr,
-                                      (int)max_pairs, 0, 64, cfg.stream);
+  e = cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const unsigned*)nullptr, (unsigned*)nullptr,
+                                      (const double*)nullptr, (double*)nullptr, (int)max_pairs, 0, 32, cfg.stream);
   if (e != cudaSuccess)
   {
     return e;
   }
-  const size_t slab = round256((size_t)max_pairs * 8);
-  unsigned char* pb = static_cast<unsigned char*>(scratch(1, 4 * slab + round256(sort_bytes)));
+  const size_t kslab = round256((size_t)max_pairs * 4);
+  const size_t pslab = round256((size_t)max_pairs * 8);
+  unsigned char* pb = static_cast<unsigned char*>(scratch(1, 2 * kslab + 2 * pslab + round256(sort_bytes)));
   if (pb == nullptr)
   {
     return cudaErrorMemoryAllocation;
   }
-  auto* keys_a = reinterpret_cast<unsigned long long*>(pb);
-  auto* keys_b = reinterpret_cast<unsigned long long*>(pb + slab);
-  auto* prods_a = reinterpret_cast<double*>(pb + 2 * slab);
-  auto* prods_b = reinterpret_cast<double*>(pb + 3 * slab);
-  void* sort_tmp = pb + 4 * slab;
+  auto* keys_a = reinterpret_cast<unsigned*>(pb);
+  auto* keys_b = reinterpret_cast<unsigned*>(pb + kslab);
+  auto* prods_a = reinterpret_cast<double*>(pb + 2 * kslab);
+  auto* prods_b = reinterpret_cast<double*>(pb + 2 * kslab + pslab);
+  void* sort_tmp = pb + 2 * kslab + 2 * pslab;
 
   // 3. chunks of whole LORs, reduced in order
-  const int enum_bits = bits_for(n);
-  const int key_bits = enum_bits + bits_for(n_vox);
+  const int key_bits = bits_for(n_vox);
   long long first = 0;
   while (first < n)
   {
@@ -295,8 +294,7 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
     if (m > 0)
     {
       k_emit<<<blocks_for(last - first, cfg.block), cfg.block, 0, cfg.stream>>>(
-        g, s, t, vals, vals_by_enum ? 1 : 0, (int)first, (int)last, offsets, off[(size_t)first], enum_bits, keys_a,
-        prods_a);
+        g, s, t, vals, vals_by_enum ? 1 : 0, (int)first, (int)last, offsets, off[(size_t)first], keys_a, prods_a);
       size_t tmp = sort_bytes;
       e = cub::DeviceRadixSort::SortPairs(sort_tmp, tmp, keys_a, keys_b, prods_a, prods_b, (int)m, 0, key_bits,
                                           cfg.stream);
@@ -304,7 +302,7 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
       {
         return e;
       }
-      k_reduce_runs<<<blocks_for(m, 256), 256, 0, cfg.stream>>>(m, keys_b, prods_b, enum_bits, img);
+      k_reduce_runs<<<blocks_for(m, 256), 256, 0, cfg.stream>>>(m, keys_b, prods_b, img);
       *launches += 2;
     }
     first = last;
