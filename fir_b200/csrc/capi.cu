@@ -597,7 +597,7 @@ void det_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, 
     }
   };
   long long launches = 0;
-  // chunks of at most det_chunk pairs (default 2^28: 8 GiB of keys,
+  // chunks of at most det_chunk pairs (default 2^28: about 6 GiB of keys,
   // products and sort buffers)
   cuda_ok(deterministic_backproject(g, s, t, vals, by_enum, img, scratch, c.det_chunk, nvox, cfg_of(c), &launches),
           "deterministic backprojection");

@@ -147,7 +147,7 @@ typedef enum fir_option
    * stream; read the accumulated device time with fir_ctx_projector_time. */
   FIR_OPT_TIMING = 5,
   /* Deterministic backprojection works on chunks of at most this many
-   * (voxel, contribution) pairs (16 bytes each, twice, plus sort space);
+   * (voxel, contribution) pairs (12 bytes each, twice, plus sort space);
    * 0 restores the default of 2^28.  Any chunk size gives the same result. */
   FIR_OPT_DETERMINISTIC_CHUNK = 6,
   /* Testing aid for failure reporting.  k > 0 bounds every traversal at k
