@@ -17,6 +17,7 @@
 // chunk, so chunking does not change the order either.
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <vector>
 
 #include "internal.h"
@@ -94,26 +95,37 @@ __global__ void __launch_bounds__(256) k_emit(Grid g, Sino s, Tables t, const fl
   });
 }
 
-// One thread per run of equal voxel: FIR's sequential accumulation.
-__global__ void k_reduce_runs(long long n, const unsigned* __restrict__ keys, const double* __restrict__ prods,
-                              float* img)
+// One warp per run of equal voxel (run r: voxel[r], products [start[r],
+// start[r] + len[r]) of the sorted array): the warp loads 32 products at a
+// time, coalesced, and every lane replays FIR's sequential accumulation
+// float(double(acc) + product) in run order through shuffles, so the lanes
+// stay converged and the order is exactly the run's.
+__global__ void __launch_bounds__(256) k_reduce_runs(const int* __restrict__ n_runs, const unsigned* __restrict__ voxel,
+                                                     const int* __restrict__ start, const int* __restrict__ len,
+                                                     const double* __restrict__ prods, float* img)
 {
-  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (j >= n)
+  const long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= *n_runs)
   {
-    return;
+    return;  // the whole warp: r is the same on every lane
   }
-  const unsigned voxel = keys[j];
-  if (j > 0 && keys[j - 1] == voxel)
+  const unsigned v = voxel[r];
+  const int first = start[r], n = len[r];
+  float acc = img[v];
+  for (int base = 0; base < n; base += 32)
   {
-    return;
+    const int k_end = n - base < 32 ? n - base : 32;
+    const double p = lane < k_end ? prods[first + base + lane] : 0.0;
+    for (int k = 0; k < k_end; ++k)
+    {
+      acc = __double2float_rn(dadd((double)acc, __shfl_sync(0xffffffffu, p, k)));
+    }
   }
-  float acc = img[voxel];
-  for (long long k = j; k < n && keys[k] == voxel; ++k)
+  if (lane == 0)
   {
-    acc = __double2float_rn(dadd((double)acc, prods[k]));
+    img[v] = acc;
   }
-  img[voxel] = acc;
 }
 
 // The ratio of one OSEM sub-iteration per enumerated LOR
@@ -260,16 +272,31 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
   {
     max_pairs = g.guard;
   }
-  size_t sort_bytes = 0;
+  // runs of one chunk: at most one per voxel and one per pair
+  const long long max_runs = max_pairs < n_vox ? max_pairs : n_vox;
+  size_t sort_bytes = 0, rle_bytes = 0, run_scan_bytes = 0;
   e = cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const unsigned*)nullptr, (unsigned*)nullptr,
                                       (const double*)nullptr, (double*)nullptr, (int)max_pairs, 0, 32, cfg.stream);
+  if (e == cudaSuccess)
+  {
+    e = cub::DeviceRunLengthEncode::Encode(nullptr, rle_bytes, (const unsigned*)nullptr, (unsigned*)nullptr,
+                                           (int*)nullptr, (int*)nullptr, (int)max_pairs, cfg.stream);
+  }
+  if (e == cudaSuccess)
+  {
+    e = cub::DeviceScan::ExclusiveSum(nullptr, run_scan_bytes, (const int*)nullptr, (int*)nullptr, (int)max_runs,
+                                      cfg.stream);
+  }
   if (e != cudaSuccess)
   {
     return e;
   }
+  const size_t tmp_bytes = std::max(sort_bytes, std::max(rle_bytes, run_scan_bytes));
   const size_t kslab = round256((size_t)max_pairs * 4);
   const size_t pslab = round256((size_t)max_pairs * 8);
-  unsigned char* pb = static_cast<unsigned char*>(scratch(1, 2 * kslab + 2 * pslab + round256(sort_bytes)));
+  const size_t rslab = round256((size_t)max_runs * 4);
+  unsigned char* pb = static_cast<unsigned char*>(
+    scratch(1, 2 * kslab + 2 * pslab + 3 * rslab + 256 + round256(tmp_bytes)));
   if (pb == nullptr)
   {
     return cudaErrorMemoryAllocation;
@@ -278,7 +305,11 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
   auto* keys_b = reinterpret_cast<unsigned*>(pb + kslab);
   auto* prods_a = reinterpret_cast<double*>(pb + 2 * kslab);
   auto* prods_b = reinterpret_cast<double*>(pb + 2 * kslab + pslab);
-  void* sort_tmp = pb + 2 * kslab + 2 * pslab;
+  auto* run_voxel = reinterpret_cast<unsigned*>(pb + 2 * kslab + 2 * pslab);
+  auto* run_len = reinterpret_cast<int*>(pb + 2 * kslab + 2 * pslab + rslab);
+  auto* run_start = reinterpret_cast<int*>(pb + 2 * kslab + 2 * pslab + 2 * rslab);
+  auto* n_runs = reinterpret_cast<int*>(pb + 2 * kslab + 2 * pslab + 3 * rslab);
+  void* sort_tmp = pb + 2 * kslab + 2 * pslab + 3 * rslab + 256;
 
   // 3. chunks of whole LORs, reduced in order
   const int key_bits = bits_for(n_vox);
@@ -295,14 +326,28 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
     {
       k_emit<<<blocks_for(last - first, cfg.block), cfg.block, 0, cfg.stream>>>(
         g, s, t, vals, vals_by_enum ? 1 : 0, (int)first, (int)last, offsets, off[(size_t)first], keys_a, prods_a);
-      size_t tmp = sort_bytes;
+      size_t tmp = tmp_bytes;
       e = cub::DeviceRadixSort::SortPairs(sort_tmp, tmp, keys_a, keys_b, prods_a, prods_b, (int)m, 0, key_bits,
                                           cfg.stream);
+      if (e == cudaSuccess)
+      {
+        tmp = tmp_bytes;
+        e = cub::DeviceRunLengthEncode::Encode(sort_tmp, tmp, keys_b, run_voxel, run_len, n_runs, (int)m, cfg.stream);
+      }
+      const long long runs_cap = m < max_runs ? m : max_runs;
+      if (e == cudaSuccess)
+      {
+        // run starts: exclusive sum of the lengths (entries past the run
+        // count are never read)
+        tmp = tmp_bytes;
+        e = cub::DeviceScan::ExclusiveSum(sort_tmp, tmp, run_len, run_start, (int)runs_cap, cfg.stream);
+      }
       if (e != cudaSuccess)
       {
         return e;
       }
-      k_reduce_runs<<<blocks_for(m, 256), 256, 0, cfg.stream>>>(m, keys_b, prods_b, img);
+      k_reduce_runs<<<blocks_for(runs_cap * 32, 256), 256, 0, cfg.stream>>>(n_runs, run_voxel, run_start, run_len,
+                                                                           prods_b, img);
       *launches += 2;
     }
     first = last;
