@@ -36,7 +36,7 @@ NVCC_FLAGS = [
     "-lineinfo",
     "--fmad=false",
     "-Xcompiler",
-    "-fPIC,-ffp-contract=off",
+    "-fPIC,-ffp-contract=off,-fvisibility=hidden",
     "--expt-relaxed-constexpr",
     "-ccbin",
     CXX,

@@ -1,0 +1,637 @@
+// C ABI of the batched OSEM (fir_batch_*, include/fir_cuda.h): many
+// independent reconstructions run as one schedule.  Kernels in batch.cu.
+#include "capi_common.h"
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+using namespace fir;
+using namespace fir::abi;
+
+// ================================================================== batches
+//
+// fir_batch: many independent OSEM reconstructions run together (see
+// batch.cu for the kernels).  The host builds, once, the per-problem device
+// descriptors and the item lists of every step of the schedule:
+//   prepare   all problems, voxel blocks          (initial cut, double copy)
+//   step t    projector items (bundles of 32 LORs), EM items (voxel blocks),
+//             filter items (voxel blocks of the problems that filter at t)
+// Items of the projector are ordered by decreasing path length, so that the
+// queue hands out the longest bundles first.
+
+struct fir_batch
+{
+  struct Problem
+  {
+    ProjInfo p;
+    VolInfo v;
+    fir_osem_params prm;
+    int n_subsets = 1;
+    int n_sub_total = 0;
+    int n_enum = 0;
+    bool filter = false;
+    double path = 0.0;  // nx + ny + nz: relative cost of a bundle
+    size_t off_sino = 0, off_sens = 0, off_img = 0, off_wide = 0, off_bp = 0, off_t1 = 0, off_t2 = 0,
+           off_xy = 0, off_z = 0;
+    DevBuf bias;
+  };
+  struct Launch
+  {
+    int item_off = 0, n_items = 0, n_units = 0;
+  };
+  struct Step
+  {
+    Launch proj, em, filt;
+  };
+
+  fir_ctx* ctx = nullptr;
+  int n = 0;
+  int n_sms = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  std::vector<Problem> pr;
+  std::vector<BatchProblem> desc_host;
+  DevBuf arena, desc, items, queue;
+  Launch all;
+  std::vector<Step> steps;
+  BatchLaunch shape{128, 0, 1};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long long schedule_launches = 0;
+};
+
+namespace
+{
+fir_batch& check_batch(fir_batch* b)
+{
+  if (b == nullptr)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "batch is NULL");
+  }
+  check_ctx(b->ctx);
+  return *b;
+}
+
+fir_batch::Problem& batch_problem(fir_batch& b, int p)
+{
+  if (p < 0 || p >= b.n)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "problem index ", p, " out of range [0, ", b.n, ")");
+  }
+  return b.pr[(size_t)p];
+}
+
+void drop_graph(fir_batch& b)
+{
+  if (b.exec != nullptr)
+  {
+    cudaGraphExecDestroy(b.exec);
+    b.exec = nullptr;
+  }
+  if (b.graph != nullptr)
+  {
+    cudaGraphDestroy(b.graph);
+    b.graph = nullptr;
+  }
+}
+
+void release_batch(fir_batch& b)
+{
+  drop_graph(b);
+  for (auto& q : b.pr)
+  {
+    q.bias.release();
+  }
+  for (DevBuf* d : {&b.arena, &b.desc, &b.items, &b.queue})
+  {
+    d->release();
+  }
+  if (b.ev_in != nullptr)
+  {
+    cudaEventDestroy(b.ev_in);
+  }
+  if (b.ev_out != nullptr)
+  {
+    cudaEventDestroy(b.ev_out);
+  }
+  if (b.stream != nullptr)
+  {
+    cudaStreamDestroy(b.stream);
+  }
+}
+
+// Appends a launch over the given problems (with per-problem subset and
+// filter flag) to the item list; units per problem from `units`.
+template<typename Units>
+fir_batch::Launch add_launch(std::vector<BatchItem>& items, const std::vector<int>& problems,
+                             const std::vector<int>& subsets, const std::vector<int>& filters, Units&& units)
+{
+  fir_batch::Launch L;
+  L.item_off = (int)items.size();
+  long long total = 0;
+  for (size_t k = 0; k < problems.size(); ++k)
+  {
+    items.push_back(BatchItem{problems[k], subsets[k], filters[k], (int)total});
+    total += units(problems[k]);
+    if (total > 0x7fffffffLL)
+    {
+      fail(FIR_ERR_NOT_SUPPORTED, "batched launch of ", total, " work units exceeds 2^31-1");
+    }
+  }
+  L.n_items = (int)problems.size();
+  L.n_units = (int)total;
+  return L;
+}
+
+void check_launch(cudaStream_t s)
+{
+  (void)s;
+  cuda_ok(cudaGetLastError(), "kernel launch");
+}
+
+// Enqueues the projector of one step (queue: that step's zeroed counter).
+void batch_project(fir_batch& b, const fir_batch::Launch& L, int* queue, const BatchLaunch& shape, cudaStream_t s)
+{
+  const auto* P = static_cast<const BatchProblem*>(b.desc.p);
+  const auto* I = static_cast<const BatchItem*>(b.items.p) + L.item_off;
+  launch_batch_project(P, I, L.n_items, L.n_units, queue, shape, b.n_sms, static_cast<int*>(b.ctx->check.p), s);
+  check_launch(s);
+}
+
+// The whole schedule on stream s; returns the number of kernel launches.
+long long batch_enqueue(fir_batch& b, cudaStream_t s)
+{
+  const auto* P = static_cast<const BatchProblem*>(b.desc.p);
+  const auto* I = static_cast<const BatchItem*>(b.items.p);
+  int* queue = static_cast<int*>(b.queue.p);
+  long long n = 0;
+  cuda_ok(cudaMemsetAsync(queue, 0, b.steps.size() * sizeof(int), s), "cudaMemsetAsync");
+  launch_batch_prepare(P, I + b.all.item_off, b.all.n_items, b.all.n_units, true, s);
+  check_launch(s);
+  ++n;
+  for (size_t t = 0; t < b.steps.size(); ++t)
+  {
+    const fir_batch::Step& st = b.steps[t];
+    batch_project(b, st.proj, queue + t, b.shape, s);
+    launch_batch_em(P, I + st.em.item_off, st.em.n_items, st.em.n_units, s);
+    check_launch(s);
+    n += 2;
+    if (st.filt.n_items > 0)
+    {
+      for (int axis = 0; axis < 3; ++axis)
+      {
+        launch_batch_filter(P, I + st.filt.item_off, st.filt.n_items, st.filt.n_units, axis, s);
+        check_launch(s);
+      }
+      n += 3;
+    }
+  }
+  return n;
+}
+
+void batch_copy(fir_batch& b, void* dst, const void* src, size_t bytes)
+{
+  cuda_ok(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, b.ctx->stream), "cudaMemcpyAsync");
+}
+
+// Orders the batch's stream after the context's stream.
+void batch_begin(fir_batch& b)
+{
+  cuda_ok(cudaEventRecord(b.ev_in, b.ctx->stream), "cudaEventRecord");
+  cuda_ok(cudaStreamWaitEvent(b.stream, b.ev_in, 0), "cudaStreamWaitEvent");
+}
+
+// Orders the context's stream after the batch's stream.
+void batch_end(fir_batch& b)
+{
+  cuda_ok(cudaEventRecord(b.ev_out, b.stream), "cudaEventRecord");
+  cuda_ok(cudaStreamWaitEvent(b.ctx->stream, b.ev_out, 0), "cudaStreamWaitEvent");
+}
+}  // namespace
+
+extern "C" {
+
+fir_status fir_batch_create(fir_batch** out, fir_ctx* ctx, int n_problems, const fir_scanner_desc* scanners,
+                            const fir_proj_desc* projs, const fir_vol_desc* vols, const fir_osem_params* params)
+{
+  return guarded(__func__, [&] {
+    if (out == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "output pointer is NULL");
+    }
+    *out = nullptr;
+    fir_ctx& c = check_ctx(ctx);
+    if (n_problems <= 0)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "a batch needs at least one problem");
+    }
+    if (scanners == nullptr || projs == nullptr || vols == nullptr || params == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "scanner, projection, volume and parameter arrays must not be NULL");
+    }
+    auto b = std::make_unique<fir_batch>();
+    b->ctx = ctx;
+    b->n = n_problems;
+    b->pr.resize((size_t)n_problems);
+    std::vector<ScannerInfo> scan((size_t)n_problems);
+    // validate and lay out the arena
+    size_t off = 0;
+    auto take = [&off](size_t bytes) {
+      const size_t at = off;
+      off += (bytes + 255) & ~(size_t)255;
+      return at;
+    };
+    for (int k = 0; k < n_problems; ++k)
+    {
+      fir_batch::Problem& q = b->pr[(size_t)k];
+      q.p = check_proj(&projs[k]);
+      q.v = check_vol(&vols[k]);
+      check_frames(q.v, 1);
+      check_osem_params(&params[k], q.p);
+      q.prm = params[k];
+      scan[(size_t)k] = scanner_tables(&scanners[k], true);
+      if (q.p.d.n_rings != scan[(size_t)k].n_rings || q.p.d.n_crystals_per_ring != scan[(size_t)k].n_cpr)
+      {
+        fail(FIR_ERR_INVALID_ARGUMENT, "problem ", k, ": Projection must have the same number of rings (",
+             scan[(size_t)k].n_rings, ") and the same number of crystals per ring (", scan[(size_t)k].n_cpr,
+             ") as the scanner");
+      }
+      q.n_subsets = q.prm.n_subsets;
+      q.n_sub_total = q.prm.n_iterations * q.prm.n_subsets;
+      q.filter = q.prm.convolution_interval > 0 && q.prm.fwhm_xyz[0] > 0.0f && q.prm.fwhm_xyz[1] > 0.0f &&
+                 q.prm.fwhm_xyz[2] > 0.0f;
+      q.path = (double)q.v.d.nx + q.v.d.ny + q.v.d.nz;
+      const size_t nv = (size_t)q.v.nvox;
+      q.off_sino = take((size_t)q.p.g.n_bins * sizeof(float));
+      q.off_sens = take(nv * q.n_subsets * sizeof(float));
+      q.off_img = take(nv * sizeof(float));
+      q.off_wide = take(nv * sizeof(double));
+      q.off_bp = take(nv * sizeof(float));
+      q.off_t1 = take(q.filter ? nv * sizeof(float) : 0);
+      q.off_t2 = take(q.filter ? nv * sizeof(float) : 0);
+      q.off_xy = take(scan[(size_t)k].xy.size() * sizeof(double));
+      q.off_z = take(scan[(size_t)k].z.size() * sizeof(double));
+    }
+    b->desc_host.resize((size_t)n_problems);
+    cuda_ok(cudaDeviceGetAttribute(&b->n_sms, cudaDevAttrMultiProcessorCount, c.device), "cudaDeviceGetAttribute");
+    try
+    {
+      cuda_ok(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+      cuda_ok(cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming), "cudaEventCreate");
+      cuda_ok(cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming), "cudaEventCreate");
+      auto* base = static_cast<unsigned char*>(b->arena.ensure(std::max<size_t>(off, 256)));
+      cuda_ok(cudaMemsetAsync(base, 0, off, c.stream), "cudaMemsetAsync");
+      for (int k = 0; k < n_problems; ++k)
+      {
+        fir_batch::Problem& q = b->pr[(size_t)k];
+        BatchProblem& d = b->desc_host[(size_t)k];
+        std::memset(&d, 0, sizeof(d));
+        fir_ctx geo;
+        geo.geometry = c.geometry;
+        d.g = grid_of(geo, q.v);
+        d.s = sino_of(q.p, q.n_subsets, 0);
+        q.n_enum = d.s.n_enum;
+        batch_copy(*b, base + q.off_xy, scan[(size_t)k].xy.data(), scan[(size_t)k].xy.size() * sizeof(double));
+        batch_copy(*b, base + q.off_z, scan[(size_t)k].z.data(), scan[(size_t)k].z.size() * sizeof(double));
+        d.t = Tables{reinterpret_cast<const double2*>(base + q.off_xy), reinterpret_cast<const double*>(base + q.off_z)};
+        d.sino = reinterpret_cast<const float*>(base + q.off_sino);
+        d.bias = nullptr;
+        d.sens = reinterpret_cast<const float*>(base + q.off_sens);
+        d.img = reinterpret_cast<float*>(base + q.off_img);
+        d.wide = reinterpret_cast<double*>(base + q.off_wide);
+        d.bp = reinterpret_cast<float*>(base + q.off_bp);
+        d.t1 = q.filter ? reinterpret_cast<float*>(base + q.off_t1) : nullptr;
+        d.t2 = q.filter ? reinterpret_cast<float*>(base + q.off_t2) : nullptr;
+        d.nvox = (int)q.v.nvox;
+        d.skip_zero = c.skip_zero;
+        d.vx = q.v.d.voxel_x;
+        d.vy = q.v.d.voxel_y;
+        d.cut = q.prm.cut_radius > 0.0f ? q.prm.cut_radius : 0.0f;
+        d.fwhm = q.prm.fwhm_xyz[0] > q.prm.fwhm_xyz[1] ? q.prm.fwhm_xyz[0] : q.prm.fwhm_xyz[1];
+        if (q.filter)
+        {
+          d.tx = gauss_taps(q.prm.fwhm_xyz[0], q.v.d.voxel_x, false);
+          d.ty = gauss_taps(q.prm.fwhm_xyz[1], q.v.d.voxel_y, false);
+          d.tz = gauss_taps(q.prm.fwhm_xyz[2], q.v.d.voxel_z, true);
+        }
+      }
+      // item lists
+      std::vector<BatchItem> items;
+      std::vector<int> all((size_t)n_problems), zeros((size_t)n_problems, 0);
+      for (int k = 0; k < n_problems; ++k)
+      {
+        all[(size_t)k] = k;
+      }
+      auto vox_units = [&](int k) { return (b->pr[(size_t)k].v.nvox + kBatchBlock - 1) / kBatchBlock; };
+      auto lor_units = [&](int k) { return ((long long)b->pr[(size_t)k].n_enum + 31) / 32; };
+      b->all = add_launch(items, all, zeros, zeros, vox_units);
+      std::vector<int> order = all;
+      std::stable_sort(order.begin(), order.end(),
+                       [&](int x, int y) { return b->pr[(size_t)x].path > b->pr[(size_t)y].path; });
+      int n_steps = 0;
+      for (const auto& q : b->pr)
+      {
+        n_steps = std::max(n_steps, q.n_sub_total);
+      }
+      for (int t = 0; t < n_steps; ++t)
+      {
+        std::vector<int> probs, subs, filts, fprobs, fsubs, fflags;
+        for (int k : order)
+        {
+          const fir_batch::Problem& q = b->pr[(size_t)k];
+          if (t >= q.n_sub_total)
+          {
+            continue;
+          }
+          const int subiter = t + 1;
+          const int f = q.filter && subiter % q.prm.convolution_interval == 0 ? 1 : 0;
+          probs.push_back(k);
+          subs.push_back(t % q.n_subsets);
+          filts.push_back(f);
+          if (f)
+          {
+            fprobs.push_back(k);
+            fsubs.push_back(t % q.n_subsets);
+            fflags.push_back(1);
+          }
+        }
+        fir_batch::Step st;
+        st.proj = add_launch(items, probs, subs, filts, lor_units);
+        st.em = add_launch(items, probs, subs, filts, vox_units);
+        st.filt = add_launch(items, fprobs, fsubs, fflags, vox_units);
+        b->steps.push_back(st);
+      }
+      b->desc.ensure(b->desc_host.size() * sizeof(BatchProblem));
+      batch_copy(*b, b->desc.p, b->desc_host.data(), b->desc_host.size() * sizeof(BatchProblem));
+      b->items.ensure(std::max<size_t>(items.size(), 1) * sizeof(BatchItem));
+      batch_copy(*b, b->items.p, items.data(), items.size() * sizeof(BatchItem));
+      b->queue.ensure(std::max<size_t>(b->steps.size(), 1) * sizeof(int));
+      cuda_ok(cudaStreamSynchronize(c.stream), "cudaStreamSynchronize");
+      b->schedule_launches = 1;
+      for (const auto& st : b->steps)
+      {
+        b->schedule_launches += 2 + (st.filt.n_items > 0 ? 3 : 0);
+      }
+    }
+    catch (...)
+    {
+      release_batch(*b);
+      throw;
+    }
+    *out = b.release();
+  });
+}
+
+fir_status fir_batch_destroy(fir_batch* batch)
+{
+  return guarded(__func__, [&] {
+    if (batch == nullptr)
+    {
+      return;
+    }
+    if (batch->ctx != nullptr)
+    {
+      cudaSetDevice(batch->ctx->device);
+    }
+    if (batch->stream != nullptr)
+    {
+      cudaStreamSynchronize(batch->stream);
+    }
+    release_batch(*batch);
+    delete batch;
+  });
+}
+
+fir_status fir_batch_set_data(fir_batch* batch, int p, const float* sino, const float* sens, const float* bias)
+{
+  return guarded(__func__, [&] {
+    fir_batch& b = check_batch(batch);
+    fir_batch::Problem& q = batch_problem(b, p);
+    if (sino == nullptr || sens == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "sinogram and sensitivity must not be NULL");
+    }
+    auto* base = static_cast<unsigned char*>(b.arena.p);
+    cuda_ok(cudaStreamSynchronize(b.stream), "cudaStreamSynchronize");
+    batch_copy(b, base + q.off_sino, sino, (size_t)q.p.g.n_bins * sizeof(float));
+    batch_copy(b, base + q.off_sens, sens, (size_t)q.v.nvox * q.n_subsets * sizeof(float));
+    BatchProblem& d = b.desc_host[(size_t)p];
+    const float* want = nullptr;
+    if (bias != nullptr)
+    {
+      want = static_cast<const float*>(q.bias.ensure((size_t)q.p.g.n_bins * sizeof(float)));
+      batch_copy(b, q.bias.p, bias, (size_t)q.p.g.n_bins * sizeof(float));
+    }
+    if (d.bias != want)
+    {
+      d.bias = want;
+      batch_copy(b, static_cast<BatchProblem*>(b.desc.p) + p, &d, sizeof(BatchProblem));
+    }
+    cuda_ok(cudaStreamSynchronize(b.ctx->stream), "cudaStreamSynchronize");
+  });
+}
+
+fir_status fir_batch_set_image(fir_batch* batch, int p, const float* img)
+{
+  return guarded(__func__, [&] {
+    fir_batch& b = check_batch(batch);
+    fir_batch::Problem& q = batch_problem(b, p);
+    if (img == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "image must not be NULL");
+    }
+    cuda_ok(cudaStreamSynchronize(b.stream), "cudaStreamSynchronize");
+    batch_copy(b, static_cast<unsigned char*>(b.arena.p) + q.off_img, img, (size_t)q.v.nvox * sizeof(float));
+    cuda_ok(cudaStreamSynchronize(b.ctx->stream), "cudaStreamSynchronize");
+  });
+}
+
+fir_status fir_batch_get_image(fir_batch* batch, int p, float* img)
+{
+  return guarded(__func__, [&] {
+    fir_batch& b = check_batch(batch);
+    fir_batch::Problem& q = batch_problem(b, p);
+    if (img == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "image must not be NULL");
+    }
+    batch_copy(b, img, static_cast<unsigned char*>(b.arena.p) + q.off_img, (size_t)q.v.nvox * sizeof(float));
+    read_checks(*b.ctx);
+  });
+}
+
+fir_status fir_batch_set_launch(fir_batch* batch, int block, int blocks_per_sm, int grab)
+{
+  return guarded(__func__, [&] {
+    fir_batch& b = check_batch(batch);
+    if (block < 32 || block > 256 || block % 32 != 0)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "block size must be a multiple of 32 in [32, 256]");
+    }
+    if (blocks_per_sm < 0 || grab < 1 || grab > 64)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "blocks per SM must be >= 0 and grab in [1, 64]");
+    }
+    const int fit = batch_max_resident(block);
+    const BatchLaunch s{block, blocks_per_sm > fit ? fit : blocks_per_sm, grab};
+    if (s.block != b.shape.block || s.blocks_per_sm != b.shape.blocks_per_sm || s.grab != b.shape.grab)
+    {
+      cuda_ok(cudaStreamSynchronize(b.stream), "cudaStreamSynchronize");
+      drop_graph(b);
+      b.shape = s;
+    }
+  });
+}
+
+fir_status fir_batch_get_launch(const fir_batch* batch, int* block, int* blocks_per_sm, int* grab)
+{
+  return guarded(__func__, [&] {
+    if (batch == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "batch is NULL");
+    }
+    if (block != nullptr)
+      *block = batch->shape.block;
+    if (blocks_per_sm != nullptr)
+      *blocks_per_sm = batch->shape.blocks_per_sm;
+    if (grab != nullptr)
+      *grab = batch->shape.grab;
+  });
+}
+
+fir_status fir_batch_schedule(const fir_batch* batch, int* n_steps, long long* n_launches)
+{
+  return guarded(__func__, [&] {
+    if (batch == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "batch is NULL");
+    }
+    if (n_steps != nullptr)
+      *n_steps = (int)batch->steps.size();
+    if (n_launches != nullptr)
+      *n_launches = batch->schedule_launches;
+  });
+}
+
+fir_status fir_batch_tune(fir_batch* batch, double* best_ms)
+{
+  return guarded(__func__, [&] {
+    fir_batch& b = check_batch(batch);
+    if (b.steps.empty())
+    {
+      if (best_ms != nullptr)
+        *best_ms = 0.0;
+      return;
+    }
+    const auto* P = static_cast<const BatchProblem*>(b.desc.p);
+    const auto* I = static_cast<const BatchItem*>(b.items.p);
+    int* queue = static_cast<int*>(b.queue.p);
+    std::vector<BatchLaunch> cand;
+    for (int block : {64, 128, 256})
+    {
+      cand.push_back(BatchLaunch{block, 0, 1});
+      const int fit = batch_max_resident(block);
+      for (int per_sm : {fit, std::max(1, fit / 2)})
+      {
+        for (int grab : {1, 2, 4})
+        {
+          cand.push_back(BatchLaunch{block, per_sm, grab});
+        }
+      }
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cuda_ok(cudaEventCreate(&e0), "cudaEventCreate");
+    cuda_ok(cudaEventCreate(&e1), "cudaEventCreate");
+    double best = 1e300;
+    BatchLaunch pick = b.shape;
+    try
+    {
+      batch_begin(b);
+      for (const BatchLaunch& L : cand)
+      {
+        double t_min = 1e300;
+        for (int rep = 0; rep < 2; ++rep)
+        {
+          launch_batch_prepare(P, I + b.all.item_off, b.all.n_items, b.all.n_units, false, b.stream);
+          check_launch(b.stream);
+          cuda_ok(cudaMemsetAsync(queue, 0, sizeof(int), b.stream), "cudaMemsetAsync");
+          cuda_ok(cudaEventRecord(e0, b.stream), "cudaEventRecord");
+          batch_project(b, b.steps[0].proj, queue, L, b.stream);
+          cuda_ok(cudaEventRecord(e1, b.stream), "cudaEventRecord");
+          cuda_ok(cudaEventSynchronize(e1), "cudaEventSynchronize");
+          float ms = 0.0f;
+          cuda_ok(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+          t_min = std::min(t_min, (double)ms);
+        }
+        if (t_min < best)
+        {
+          best = t_min;
+          pick = L;
+        }
+      }
+      batch_end(b);
+    }
+    catch (...)
+    {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b.ctx->launches += (long long)cand.size() * 4;
+    if (pick.block != b.shape.block || pick.blocks_per_sm != b.shape.blocks_per_sm || pick.grab != b.shape.grab)
+    {
+      drop_graph(b);
+      b.shape = pick;
+    }
+    if (best_ms != nullptr)
+    {
+      *best_ms = best;
+    }
+    read_checks(*b.ctx);
+  });
+}
+
+fir_status fir_batch_osem(fir_batch* batch, int use_graph)
+{
+  return guarded(__func__, [&] {
+    fir_batch& b = check_batch(batch);
+    batch_begin(b);
+    if (use_graph)
+    {
+      if (b.exec == nullptr)
+      {
+        cuda_ok(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+        try
+        {
+          batch_enqueue(b, b.stream);
+        }
+        catch (...)
+        {
+          cudaGraph_t g = nullptr;
+          cudaStreamEndCapture(b.stream, &g);
+          if (g != nullptr)
+          {
+            cudaGraphDestroy(g);
+          }
+          cudaGetLastError();
+          throw;
+        }
+        cuda_ok(cudaStreamEndCapture(b.stream, &b.graph), "cudaStreamEndCapture");
+        cuda_ok(cudaGraphInstantiate(&b.exec, b.graph, 0), "cudaGraphInstantiate");
+      }
+      cuda_ok(cudaGraphLaunch(b.exec, b.stream), "cudaGraphLaunch");
+    }
+    else
+    {
+      batch_enqueue(b, b.stream);
+    }
+    batch_end(b);
+    b.ctx->launches += b.schedule_launches;
+  });
+}
+
+}  // extern "C"

@@ -49,6 +49,12 @@
 extern "C" {
 #endif
 
+/* The library is built with hidden visibility; these entry points are its
+ * exported interface. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
 #define FIR_CUDA_ABI_VERSION 1
 
 typedef enum fir_status
@@ -423,6 +429,10 @@ fir_status fir_siddon_paths(fir_ctx* ctx, const fir_vol_desc* vol, long long n, 
 fir_status fir_lor_paths(fir_ctx* ctx, const fir_proj_desc* proj, const fir_vol_desc* vol,
                          long long n, const long long* bins, int cap, int* coords, double* lengths,
                          int* counts, int* crosses);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
 
 #ifdef __cplusplus
 }
