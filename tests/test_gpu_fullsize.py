@@ -1,7 +1,8 @@
-"""The clinical workload at full size (32 rings x 512 crystals, 3.28e7 LORs,
-200x200x64 image at 3 mm) against FIR itself, compiled from its sources and
-run on the host's cores:
-* the forward projection of the phantom equals FIR's on every bin;
+"""The clinical workload at full size (32 rings x 512 crystals, 200x200x64
+image at 3 mm; 3.28e7 LORs, and 1.34e8 in its full-FOV form) against FIR
+itself, compiled from its sources and run on the host's cores:
+* the forward projection of the phantom equals FIR's on every bin, in both
+  forms;
 * one full OSEM iteration (16 subsets, FWHM 4 mm filter, cut radius) from
   the same data and sensitivity agrees with FIR's to 1e-4 relative L2.
 """
@@ -51,3 +52,17 @@ def test_clinical_osem_iteration_matches_fir(clinical, reference):
                           sens.cpu().numpy(), prm)
     assert float(want.max()) > 0
     assert np.linalg.norm(got - want) <= 1e-4 * np.linalg.norm(want)
+
+
+def test_clinical_full_fov_forward_bit_identical_to_fir(gpu_ctx_factory, reference):
+    """All 511 tangential bins (1.34e8 LORs, the '~1e8 LORs' form of the
+    clinical configuration): every bin equals FIR's."""
+    reference.threads(os.cpu_count() or 1)
+    w = workloads.clinical(full_fov=True)
+    ctx = gpu_ctx_factory(w.scanner)
+    x = workloads.activity(w)
+    got = torch.empty(w.n_lors, device=DEV)
+    ctx.forward(w.vol, torch.from_numpy(x).to(DEV), w.proj, got)
+    torch.cuda.synchronize()
+    want = reference.forward(w.scanner, w.proj, w.vol, x, w.n_lors)
+    np.testing.assert_array_equal(got.cpu().numpy(), want)
