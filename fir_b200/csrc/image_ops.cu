@@ -51,18 +51,19 @@ __global__ void k_widen(long long n, const float* __restrict__ in, double* __res
 __global__ void k_conv_pass(int nx, int ny, int nz, int axis, Taps taps, const float* __restrict__ in,
                             float* __restrict__ out)
 {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long n = (long long)nx * ny * nz;
-  if (i >= n)
+  // volumes hold fewer than 2^31 voxels (checked on the host), so the
+  // coordinates come from 32-bit divisions
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nx * ny * nz)
   {
     return;
   }
-  const int x = (int)(i % nx);
-  const int y = (int)((i / nx) % ny);
-  const int z = (int)(i / ((long long)nx * ny));
+  const int x = i % nx;
+  const int y = (i / nx) % ny;
+  const int z = i / (nx * ny);
   const int coord = axis == 0 ? x : (axis == 1 ? y : z);
   const int len = axis == 0 ? nx : (axis == 1 ? ny : nz);
-  const long long stride = axis == 0 ? 1 : (axis == 1 ? (long long)nx : (long long)nx * ny);
+  const int stride = axis == 0 ? 1 : (axis == 1 ? nx : nx * ny);
   float sum = 0.0f, norm = 0.0f;
   for (int k = -taps.half; k <= taps.half; ++k)
   {
@@ -83,13 +84,13 @@ __global__ void k_conv_pass(int nx, int ny, int nz, int axis, Taps taps, const f
 __global__ void k_conv_restore(int nx, int ny, int nz, double vx, double vy, float cut, float fwhm,
                                const float* __restrict__ copy, float* __restrict__ img)
 {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)nx * ny * nz)
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nx * ny * nz)
   {
     return;
   }
-  const int x = (int)(i % nx);
-  const int y = (int)((i / nx) % ny);
+  const int x = i % nx;
+  const int y = (i / nx) % ny;
   // cutRadius - 5.0 * fwhm: float cut radius widened, double product.
   if (radius_of(x, y, nx, ny, vx, vy) >= __dsub_rn((double)cut, __dmul_rn(5.0, (double)fwhm)))
   {
@@ -99,13 +100,13 @@ __global__ void k_conv_restore(int nx, int ny, int nz, double vx, double vy, flo
 
 __global__ void k_cut_circle(int nx, int ny, int nz, double vx, double vy, float cut, float* img)
 {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)nx * ny * nz)
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nx * ny * nz)
   {
     return;
   }
-  const int x = (int)(i % nx);
-  const int y = (int)((i / nx) % ny);
+  const int x = i % nx;
+  const int y = (i / nx) % ny;
   if (radius_of(x, y, nx, ny, vx, vy) > (double)cut)
   {
     img[i] = 0.0f;
