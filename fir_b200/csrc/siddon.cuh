@@ -387,13 +387,89 @@ __device__ __forceinline__ double walk_step(Walk& w, double prev, bool& more, Em
   return next;
 }
 
+// Advances left in each dimension, from the linear index (every index is
+// inside the volume when this is called).
+__device__ __forceinline__ void left_from_index(const Grid& g, Walk& w)
+{
+  const int z = w.c / g.nxy;
+  const int rest = w.c - z * g.nxy;
+  const int y = rest / g.nx;
+  const int idx[3] = {rest - y * g.nx, y, z};
+  const int n[3] = {g.nx, g.ny, g.nz};
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    w.left[d] = w.step[d] > 0 ? n[d] - 1 - idx[d] : idx[d];
+  }
+}
+
 // With the fast tie form every alpha is finite or +inf and >= EPS, and
 // alphaMax <= 1, so every step either advances the dimension that attains
 // the minimum (using up one of its finitely many advances) or reaches
-// alphaMax: the loop ends without a step bound.  Two steps per trip.
+// alphaMax: the loop ends without a step bound.
+//
+// Most steps are far from any index leaving the volume, and those need
+// neither the advance counts nor the alphaMax select.  Dimension d leaves
+// the volume at its (left_d + 1)-th crossing, at alpha X_d = a_d + left_d
+// da_d (accumulated by repeated addition; the closed form differs from the
+// sum by at most (left_d + 2) ulp(X_d), far below X_d 2^-20).  A step
+// advances that crossing only if X_d < ru(next + EPS), so while next <
+// X_d - EPS - X_d 2^-20 for every d, and next < alphaMax, no index leaves
+// and next is the minimum alpha.  Those steps run first without the
+// bookkeeping; the advance counts are then rebuilt from the linear index
+// and the checked steps finish the walk.  Two steps per trip in both.
 template<class Emit>
-__device__ __forceinline__ void walk_loop_fast(Walk& w, double& prev, bool active, Emit&& emit)
+__device__ __forceinline__ void walk_loop_fast(const Grid& g, Walk& w, double& prev, bool active, Emit&& emit)
 {
+  double end = w.amax;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    const double x = w.left[d] > 0 ? dadd(w.a[d], dmul((double)w.left[d], w.da[d])) : w.a[d];
+    const double lim = dsub(dsub(x, kEps), dmul(x, 0x1p-20));
+    end = (lim < end || lim != lim) ? lim : end;  // a NaN bound leaves every step to the checked loop
+  }
+  if (active)
+  {
+    while (true)
+    {
+      double m = min_of(w.a[0], min_of(w.a[1], w.a[2]));
+      if (!(m < end))
+      {
+        break;
+      }
+      emit(true, w.c, dmul(dsub(m, prev), w.d12));
+      double thr = __dadd_ru(m, kEps);
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+      {
+        if (w.a[d] < thr)
+        {
+          w.a[d] = dadd(w.a[d], w.da[d]);
+          w.c += w.step[d];
+        }
+      }
+      prev = m;
+      m = min_of(w.a[0], min_of(w.a[1], w.a[2]));
+      if (!(m < end))
+      {
+        break;
+      }
+      emit(true, w.c, dmul(dsub(m, prev), w.d12));
+      thr = __dadd_ru(m, kEps);
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+      {
+        if (w.a[d] < thr)
+        {
+          w.a[d] = dadd(w.a[d], w.da[d]);
+          w.c += w.step[d];
+        }
+      }
+      prev = m;
+    }
+    left_from_index(g, w);
+  }
   bool more = active;
   while (more)
   {
@@ -439,7 +515,7 @@ __device__ __forceinline__ bool siddon_walk(const Grid& g, Walk w, bool go, Emit
     !active || (!g.exact_only && min_of(w.amin, min_of(w.a[0], min_of(w.a[1], w.a[2]))) >= kEps);
   if (__all_sync(__activemask(), fast))
   {
-    walk_loop_fast(w, prev, active, emit);
+    walk_loop_fast(g, w, prev, active, emit);
   }
   else
   {
