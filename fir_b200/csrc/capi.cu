@@ -472,22 +472,6 @@ void det_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, 
   c.launches += launches;
 }
 
-// bp (zeroed by the caller) += backprojection of sino / (projection of the
-// widened image + bias) over the subset of s: the fused kernel, or in
-// deterministic mode the ratio kernel followed by the ordered scatter.
-void ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, const double* wimg,
-                       const float* sino, const float* mult, const float* bias, float* bp, long long nvox)
-{
-  if (c.backproj == FIR_BACKPROJ_DETERMINISTIC)
-  {
-    float* ratio = static_cast<float*>(c.ratio.ensure((size_t)std::max(s.n_enum, 1) * sizeof(float)));
-    timed_launch(c, [&] { launch_ratio(g, s, t, wimg, sino, mult, bias, ratio, cfg_of(c)); });
-    det_backproject(c, g, s, t, ratio, true, bp, nvox);
-    return;
-  }
-  timed_launch(c, [&] { launch_osem_subset(g, s, t, wimg, sino, mult, bias, bp, c.skip_zero != 0, cfg_of(c)); });
-}
-
 // Double copy of a float image in context scratch, for the projector gathers.
 const double* widen(fir_ctx& c, const float* img, long long n)
 {
@@ -495,6 +479,46 @@ const double* widen(fir_ctx& c, const float* img, long long n)
   launch_widen(n, img, d, cfg_of(c));
   after_launch(c);
   return d;
+}
+
+// bp (zeroed by the caller) += backprojection of sino / (projection of img +
+// bias) over the subset of s: the fused kernel, or in deterministic mode the
+// ratio kernel followed by the ordered scatter.  The fused kernel reads and
+// accumulates LORs that run mostly along x in images with x and y exchanged
+// (double copy and accumulator in context scratch); the accumulator is added
+// back into bp after the kernel.
+void ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, const float* img,
+                       const float* sino, const float* mult, const float* bias, float* bp, long long nvox)
+{
+  if (c.backproj == FIR_BACKPROJ_DETERMINISTIC)
+  {
+    const double* wimg = widen(c, img, nvox);
+    float* ratio = static_cast<float*>(c.ratio.ensure((size_t)std::max(s.n_enum, 1) * sizeof(float)));
+    timed_launch(c, [&] { launch_ratio(g, s, t, wimg, sino, mult, bias, ratio, cfg_of(c)); });
+    det_backproject(c, g, s, t, ratio, true, bp, nvox);
+    return;
+  }
+  if ((g.ny + 31) / 32 > 65535)
+  {
+    // beyond the tile grid of the exchange kernels: one orientation
+    const double* wimg = widen(c, img, nvox);
+    timed_launch(c, [&] {
+      launch_osem_subset(g, s, t, wimg, nullptr, sino, mult, bias, bp, nullptr, c.skip_zero != 0, cfg_of(c));
+    });
+    return;
+  }
+  const size_t n = (size_t)nvox;
+  double* wimg = static_cast<double*>(c.wide.ensure(n * sizeof(double)));
+  double* wimg_t = static_cast<double*>(c.wide_t.ensure(n * sizeof(double)));
+  float* bp_t = static_cast<float*>(c.bp_t.ensure(n * sizeof(float)));
+  cuda_ok(cudaMemsetAsync(bp_t, 0, n * sizeof(float), c.stream), "cudaMemsetAsync");
+  launch_widen_oriented(g.nx, g.ny, g.nz, img, wimg, wimg_t, cfg_of(c));
+  after_launch(c);
+  timed_launch(c, [&] {
+    launch_osem_subset(g, s, t, wimg, wimg_t, sino, mult, bias, bp, bp_t, c.skip_zero != 0, cfg_of(c));
+  });
+  launch_merge_oriented(g.nx, g.ny, g.nz, bp, bp_t, cfg_of(c));
+  after_launch(c);
 }
 
 Tables tables_of(fir_ctx& c, const ProjInfo& p)
@@ -838,8 +862,7 @@ void osem_subiteration_device(fir_ctx& c, const ProjInfo& p, const Tables& t, co
   float* bp = static_cast<float*>(c.bp.ensure((size_t)v.nvox * sizeof(float)));
   cuda_ok(cudaMemsetAsync(bp, 0, (size_t)v.nvox * sizeof(float), c.stream), "cudaMemsetAsync");
   const Sino s = sino_of(p, prm->n_subsets, subset);
-  const double* wimg = widen(c, img, v.nvox);
-  ratio_backproject(c, g, s, t, wimg, sino, mult, bias, bp, v.nvox);
+  ratio_backproject(c, g, s, t, img, sino, mult, bias, bp, v.nvox);
   launch_em_update(v.nvox, img, bp, sens_frame, cfg_of(c));
   after_launch(c);
   const bool conv = prm->convolution_interval > 0 && prm->fwhm_xyz[0] > 0.0 && prm->fwhm_xyz[1] > 0.0 &&
@@ -865,8 +888,7 @@ void osem_psf_subiteration_device(fir_ctx& c, const ProjInfo& p, const Tables& t
   cuda_ok(cudaMemcpyAsync(blur, img, bytes, cudaMemcpyDeviceToDevice, c.stream), "cudaMemcpyAsync");
   convolve_device(c, v, blur, prm->fwhm_xyz, prm->cut_radius);
   const Sino s = sino_of(p, prm->n_subsets, subset);
-  const double* wimg = widen(c, blur, v.nvox);
-  ratio_backproject(c, g, s, t, wimg, sino, mult, bias, bp, v.nvox);
+  ratio_backproject(c, g, s, t, blur, sino, mult, bias, bp, v.nvox);
   convolve_device(c, v, bp, prm->fwhm_xyz, prm->cut_radius);
   launch_em_update(v.nvox, img, bp, sens_frame, cfg_of(c));
   after_launch(c);
@@ -1599,8 +1621,7 @@ fir_status fir_ratio_backprojection(fir_ctx* ctx, const fir_proj_desc* proj, con
     float* dbp = st.out(bp, v.nvox);
     cuda_ok(cudaMemsetAsync(dbp, 0, (size_t)v.nvox * sizeof(float), c.stream), "cudaMemsetAsync");
     const Sino s = sino_of(p, n_subsets, subset);
-    const double* wimg = widen(c, dimg, v.nvox);
-    ratio_backproject(c, g, s, t, wimg, dsino, nullptr, dbias, dbp, v.nvox);
+    ratio_backproject(c, g, s, t, dimg, dsino, nullptr, dbias, dbp, v.nvox);
     finish(c, st);
   });
 }
@@ -1984,7 +2005,7 @@ extern "C" fir_status fir_osem_subiteration_noalloc(const fir_proj_desc* proj, c
     // the accumulator keeps the previous call's sums: clear it
     cuda_ok(cudaMemsetAsync(bp, 0, (size_t)v.nvox * sizeof(float), st), "cudaMemsetAsync");
     launch_widen(v.nvox, img, wide, cfg);
-    launch_osem_subset(g, s, t, wide, sino, nullptr, bias, bp, false, cfg);
+    launch_osem_subset(g, s, t, wide, nullptr, sino, nullptr, bias, bp, nullptr, false, cfg);
     launch_em_update(v.nvox, img, bp, sens_frame, cfg);
     const float* fwhm = params->fwhm_xyz;
     const bool conv = params->convolution_interval > 0 && fwhm[0] > 0.0 && fwhm[1] > 0.0 && fwhm[2] > 0.0;

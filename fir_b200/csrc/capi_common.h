@@ -157,6 +157,7 @@ struct fir_ctx
   int* check_host = nullptr;  // pinned mirror
 
   fir::abi::DevBuf bp, conv1, conv2, conv_copy, mu, wide, det, det_pairs, ratio, frames_il, frames_acc, psf_blur, psf_sens, rebin;
+  fir::abi::DevBuf wide_t, bp_t;  // x/y-exchanged double image and accumulator of the fused kernel
   std::vector<fir::abi::DevBuf> staging;
 
   // pipelined input of fir_osem from pinned host memory

@@ -45,6 +45,85 @@ __global__ void k_widen(long long n, const float* __restrict__ in, double* __res
   }
 }
 
+// The two orientations of the projector's images move through 32 x 32
+// tiles of one plane in shared memory, so that both layouts are read and
+// written in whole rows.
+constexpr int kTile = 32;
+constexpr int kTileRows = 8;
+
+// out[z][y][x] = in[z][y][x] and out_t[z][x][y] = in[z][y][x], widened to
+// double (exact).
+__global__ void __launch_bounds__(kTile * kTileRows) k_widen_oriented(int nx, int ny, int nz,
+                                                                      const float* __restrict__ in,
+                                                                      double* __restrict__ out,
+                                                                      double* __restrict__ out_t)
+{
+  __shared__ float tile[kTile][kTile + 1];
+  const int x0 = blockIdx.x * kTile, y0 = blockIdx.y * kTile;
+  for (int z = blockIdx.z; z < nz; z += gridDim.z)
+  {
+    const size_t plane = (size_t)nx * ny * z;
+    for (int j = threadIdx.y; j < kTile; j += kTileRows)
+    {
+      const int x = x0 + threadIdx.x, y = y0 + j;
+      if (x < nx && y < ny)
+      {
+        const size_t k = plane + (size_t)y * nx + x;
+        const float v = in[k];
+        out[k] = (double)v;
+        tile[j][threadIdx.x] = v;
+      }
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < kTile; j += kTileRows)
+    {
+      const int y = y0 + threadIdx.x, x = x0 + j;
+      if (x < nx && y < ny)
+      {
+        out_t[plane + (size_t)x * ny + y] = (double)tile[threadIdx.x][j];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// bp[z][y][x] += bp_t[z][x][y] (one float addition per voxel).
+__global__ void __launch_bounds__(kTile * kTileRows) k_merge_oriented(int nx, int ny, int nz, float* __restrict__ bp,
+                                                                      const float* __restrict__ bp_t)
+{
+  __shared__ float tile[kTile][kTile + 1];
+  const int x0 = blockIdx.x * kTile, y0 = blockIdx.y * kTile;
+  for (int z = blockIdx.z; z < nz; z += gridDim.z)
+  {
+    const size_t plane = (size_t)nx * ny * z;
+    for (int j = threadIdx.y; j < kTile; j += kTileRows)
+    {
+      const int x = x0 + j, y = y0 + threadIdx.x;
+      if (x < nx && y < ny)
+      {
+        tile[j][threadIdx.x] = bp_t[plane + (size_t)x * ny + y];
+      }
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < kTile; j += kTileRows)
+    {
+      const int y = y0 + j, x = x0 + threadIdx.x;
+      if (x < nx && y < ny)
+      {
+        const size_t k = plane + (size_t)y * nx + x;
+        bp[k] = __fadd_rn(bp[k], tile[threadIdx.x][j]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+dim3 plane_tiles(int nx, int ny, int nz)
+{
+  return dim3((unsigned)((nx + kTile - 1) / kTile), (unsigned)((ny + kTile - 1) / kTile),
+              (unsigned)(nz < 65535 ? nz : 65535));
+}
+
 // One pass of operations::convolve (operations.cc:84-156): sum and weight
 // norm over the in-bounds taps, accumulated in float in tap order, then
 // sum / norm.
@@ -242,6 +321,23 @@ void launch_widen(long long n, const float* in, double* out, const LaunchCfg& cf
   if (n > 0)
   {
     k_widen<<<blocks_for(n), kBlock, 0, cfg.stream>>>(n, in, out);
+  }
+}
+
+void launch_widen_oriented(int nx, int ny, int nz, const float* in, double* out, double* out_t,
+                           const LaunchCfg& cfg)
+{
+  if ((long long)nx * ny * nz > 0)
+  {
+    k_widen_oriented<<<plane_tiles(nx, ny, nz), dim3(kTile, kTileRows), 0, cfg.stream>>>(nx, ny, nz, in, out, out_t);
+  }
+}
+
+void launch_merge_oriented(int nx, int ny, int nz, float* bp, const float* bp_t, const LaunchCfg& cfg)
+{
+  if ((long long)nx * ny * nz > 0)
+  {
+    k_merge_oriented<<<plane_tiles(nx, ny, nz), dim3(kTile, kTileRows), 0, cfg.stream>>>(nx, ny, nz, bp, bp_t);
   }
 }
 

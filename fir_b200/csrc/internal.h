@@ -36,9 +36,11 @@ void launch_backward(const Grid& g, const Sino& s, const Tables& t, const float*
                      bool skip_zero, const LaunchCfg& cfg);
 // mult: per-bin multiplicative factors of the ordinary-Poisson model, or
 // nullptr for FIR's model.
-void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const double* img,
-                        const float* sino, const float* mult, const float* bias, float* bp, bool skip_zero,
-                        const LaunchCfg& cfg);
+// img_t / bp_t: the image and the accumulator with x and y exchanged (both
+// or neither); LORs running mostly along x use them.
+void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const double* img, const double* img_t,
+                        const float* sino, const float* mult, const float* bias, float* bp, float* bp_t,
+                        bool skip_zero, const LaunchCfg& cfg);
 void launch_siddon_paths(const Grid& g, long long n, const double* ends, int cap, int* coords,
                          double* lengths, int* counts, int* crosses, const LaunchCfg& cfg);
 void launch_lor_paths(const Grid& g, const Sino& s, const Tables& t, long long n,
@@ -72,6 +74,12 @@ struct Taps
 void launch_em_update(long long n, float* img, float* bp, const float* sens, const LaunchCfg& cfg);
 // Exact widening of a float image to double for the projector gathers.
 void launch_widen(long long n, const float* in, double* out, const LaunchCfg& cfg);
+// Double copies of an [nz][ny][nx] image: out in the same layout, out_t as
+// [nz][nx][ny].
+void launch_widen_oriented(int nx, int ny, int nz, const float* in, double* out, double* out_t,
+                           const LaunchCfg& cfg);
+// bp[z][y][x] += bp_t[z][x][y].
+void launch_merge_oriented(int nx, int ny, int nz, float* bp, const float* bp_t, const LaunchCfg& cfg);
 // One separable pass of operations::convolve along axis (0=x, 1=y, 2=z).
 void launch_conv_pass(int nx, int ny, int nz, int axis, const Taps& taps, const float* in, float* out,
                       const LaunchCfg& cfg);

@@ -26,20 +26,24 @@ __device__ __forceinline__ void flag(int* check, int bit)
 // kWeighted: the ordinary-Poisson model with multiplicative factors m
 // (attenuation, normalisation) per bin: estimate m * line + bias, and the
 // backprojected value m * measured / estimate.  Without it the body is FIR's.
+//
+// img_t and bp_t (both given, or both null) are the same images with x and
+// y exchanged.  A LOR that runs mostly along x gathers from img_t and adds
+// into bp_t: the 32 parallel LORs of a warp are then offset along the
+// contiguous axis, so each warp-wide gather and atomic touches about half as
+// many cache lines.  The caller adds bp_t back into bp.
 template<bool kWeighted>
 __device__ __forceinline__ void osem_lor_body(const Grid& g, const Sino& s, int subset, const Tables& t,
-                                              const double* __restrict__ img, const float* __restrict__ sino,
-                                              const float* __restrict__ mult, const float* __restrict__ bias,
-                                              float* bp, bool skip_zero, int i, int* check)
+                                              const double* __restrict__ img, const double* __restrict__ img_t,
+                                              const float* __restrict__ sino, const float* __restrict__ mult,
+                                              const float* __restrict__ bias, float* bp, float* bp_t,
+                                              bool skip_zero, int i, int* check)
 {
-  // bp may come from a descriptor in memory, not a kernel parameter: without
-  // this the compiler cannot tell the atomic's address space and tests it at
-  // every step.
-  __builtin_assume(__isGlobal(bp));
   const bool valid = i < s.n_enum;
   Lor l{};
   Walk w{};
   bool go = false;
+  bool tr = false;
   float y = 0.0f;
   if (valid)
   {
@@ -51,14 +55,21 @@ __device__ __forceinline__ void osem_lor_body(const Grid& g, const Sino& s, int 
     {
       double e[6];
       lor_ends(s, t, l, e);
-      go = siddon_setup(g, e, w);
+      tr = img_t != nullptr && fabs(dsub(e[3], e[0])) > fabs(dsub(e[4], e[1]));
+      go = siddon_setup(g, e, w, tr);
     }
   }
+  const double* im = tr ? img_t : img;
+  float* b = tr ? bp_t : bp;
+  // b may come from a descriptor in memory, not a kernel parameter: without
+  // this the compiler cannot tell the atomic's address space and tests it at
+  // every step.
+  __builtin_assume(__isGlobal(b));
   float line = 0.0f;
   bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
     if (inside)
     {
-      line = accumulate(line, len, __ldg(img + c));
+      line = accumulate(line, len, __ldg(im + c));
     }
   });
   __syncwarp();
@@ -81,7 +92,7 @@ __device__ __forceinline__ void osem_lor_body(const Grid& g, const Sino& s, int 
   ok = siddon_walk(g, w, back, [&](bool inside, int c, double len) {
          if (inside)
          {
-           atomicAdd(bp + c, __double2float_rn(dmul(len, ratio)));
+           atomicAdd(b + c, __double2float_rn(dmul(len, ratio)));
          }
        }) && ok;
   if (!ok)
@@ -95,6 +106,6 @@ __device__ __forceinline__ void osem_lor(const Grid& g, const Sino& s, int subse
                                          const float* __restrict__ bias, float* bp, bool skip_zero, int i,
                                          int* check)
 {
-  osem_lor_body<false>(g, s, subset, t, img, sino, nullptr, bias, bp, skip_zero, i, check);
+  osem_lor_body<false>(g, s, subset, t, img, nullptr, sino, nullptr, bias, bp, nullptr, skip_zero, i, check);
 }
 }  // namespace fir

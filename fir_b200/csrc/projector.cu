@@ -102,13 +102,14 @@ __global__ void __launch_bounds__(256) k_backward(Grid g, Sino s, Tables t,
 template<bool kWeighted>
 __global__ void __launch_bounds__(256, 4) k_osem_subset(Grid g, Sino s, Tables t,
                                                         const double* __restrict__ img,
+                                                        const double* __restrict__ img_t,
                                                         const float* __restrict__ sino,
                                                         const float* __restrict__ mult,
-                                                        const float* __restrict__ bias, float* bp,
+                                                        const float* __restrict__ bias, float* bp, float* bp_t,
                                                         int skip_zero, int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  osem_lor_body<kWeighted>(g, s, s.subset, t, img, sino, mult, bias, bp, skip_zero != 0, i, check);
+  osem_lor_body<kWeighted>(g, s, s.subset, t, img, img_t, sino, mult, bias, bp, bp_t, skip_zero != 0, i, check);
 }
 
 // Path dump of one segment into row i of coords / lengths.
@@ -219,24 +220,29 @@ void launch_backward(const Grid& g, const Sino& s, const Tables& t, const float*
     g, s, t, sino, img, skip_zero ? 1 : 0, cfg.check);
 }
 
-void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const double* img,
-                        const float* sino, const float* mult, const float* bias, float* bp, bool skip_zero,
-                        const LaunchCfg& cfg)
+void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const double* img, const double* img_t,
+                        const float* sino, const float* mult, const float* bias, float* bp, float* bp_t,
+                        bool skip_zero, const LaunchCfg& cfg)
 {
   if (s.n_enum == 0)
   {
     return;
   }
+  if (img_t == nullptr || bp_t == nullptr)
+  {
+    img_t = nullptr;
+    bp_t = nullptr;
+  }
   const unsigned nb = blocks_for(s.n_enum, cfg.block);
   if (mult != nullptr)
   {
-    k_osem_subset<true><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, sino, mult, bias, bp, skip_zero ? 1 : 0,
-                                                          cfg.check);
+    k_osem_subset<true><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, img_t, sino, mult, bias, bp, bp_t,
+                                                          skip_zero ? 1 : 0, cfg.check);
   }
   else
   {
-    k_osem_subset<false><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, sino, nullptr, bias, bp, skip_zero ? 1 : 0,
-                                                           cfg.check);
+    k_osem_subset<false><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, img_t, sino, nullptr, bias, bp, bp_t,
+                                                           skip_zero ? 1 : 0, cfg.check);
   }
 }
 

@@ -240,13 +240,16 @@ struct Walk
   int left[3];   // advances left before the index leaves the volume
   int step[3];   // change of the linear index per advance
   int c;         // linear index of the current voxel
+  int tr;        // 1: index of the layout with x and y exchanged, [z][x][y]
   double amin, amax, d12;
 };
 
 // Siddon::computePath setup (Siddon.cc:112-203 with dimSetup :260-317,
 // getEntryExit :319-334, getStartInd :336-350, prepareDim :352-377).
-// Returns false when the segment misses the volume.
-__device__ __forceinline__ bool siddon_setup(const Grid& g, const double e[6], Walk& w)
+// Returns false when the segment misses the volume.  With transpose the
+// linear index is that of the image with x and y exchanged ([z][x][y]); the
+// traversal itself is the same.
+__device__ __forceinline__ bool siddon_setup(const Grid& g, const double e[6], Walk& w, bool transpose = false)
 {
   double diff[3], smin[3], smax[3], snext[3];
   int dir[3];
@@ -298,7 +301,8 @@ __device__ __forceinline__ bool siddon_setup(const Grid& g, const double e[6], W
     return false;
   }
   const int n[3] = {g.nx, g.ny, g.nz};
-  const int stride[3] = {1, g.nx, g.nxy};
+  const int stride[3] = {transpose ? g.ny : 1, transpose ? 1 : g.nx, g.nxy};
+  w.tr = transpose ? 1 : 0;
 #pragma unroll
   for (int d = 0; d < 3; ++d)
   {
@@ -393,8 +397,9 @@ __device__ __forceinline__ void left_from_index(const Grid& g, Walk& w)
 {
   const int z = w.c / g.nxy;
   const int rest = w.c - z * g.nxy;
-  const int y = rest / g.nx;
-  const int idx[3] = {rest - y * g.nx, y, z};
+  const int slow = rest / (w.tr ? g.ny : g.nx);
+  const int fast = rest - slow * (w.tr ? g.ny : g.nx);
+  const int idx[3] = {w.tr ? slow : fast, w.tr ? fast : slow, z};
   const int n[3] = {g.nx, g.ny, g.nz};
 #pragma unroll
   for (int d = 0; d < 3; ++d)
