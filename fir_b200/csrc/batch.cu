@@ -66,7 +66,8 @@ __global__ void __launch_bounds__(256, 4) k_batch_osem(const BatchProblem* __res
       const int subset = __ldg(&items[it].subset);
       const BatchProblem& pb = P[p];
       const int i = (k - __ldg(&items[it].unit_begin)) * 32 + lane;
-      osem_lor(pb.g, pb.s, subset, pb.t, pb.wide, pb.sino, pb.bias, pb.bp, pb.skip_zero != 0, i, check);
+      osem_lor(pb.g, pb.s, subset, pb.t, pb.wide, pb.wide_t, pb.sino, pb.bias, pb.bp, pb.bp_t, pb.skip_zero != 0, i,
+               check);
     }
     if (!kPersistent)
     {
@@ -95,6 +96,15 @@ __device__ __forceinline__ Voxel voxel_of(const BatchProblem* P, const BatchItem
     v.j = -1;
   }
   return v;
+}
+
+// Index of voxel j in the layout with x and y exchanged.
+__device__ __forceinline__ int exchanged(const BatchProblem& pb, int j)
+{
+  const int x = j % pb.g.nx;
+  const int r = j / pb.g.nx;
+  const int y = r % pb.g.ny;
+  return (r / pb.g.ny * pb.g.nx + x) * pb.g.ny + y;
 }
 
 __device__ __forceinline__ double radius_at(const BatchProblem& pb, int j)
@@ -127,6 +137,12 @@ __global__ void __launch_bounds__(kBatchBlock) k_batch_prepare(const BatchProble
   }
   pb.wide[v.j] = (double)x;
   pb.bp[v.j] = 0.0f;
+  if (pb.wide_t != nullptr)
+  {
+    const int jt = exchanged(pb, v.j);
+    pb.wide_t[jt] = (double)x;
+    pb.bp_t[jt] = 0.0f;
+  }
 }
 
 // reconAlgos.cc:161-166 (VolData::operator/= then operator*=, VolData.cc:
@@ -141,12 +157,17 @@ __global__ void __launch_bounds__(kBatchBlock) k_batch_em(const BatchProblem* __
     return;
   }
   const BatchProblem& pb = *v.pb;
-  const float b = pb.bp[v.j];
+  const int jt = pb.bp_t != nullptr ? exchanged(pb, v.j) : -1;
+  const float b = jt >= 0 ? __fadd_rn(pb.bp[v.j], pb.bp_t[jt]) : pb.bp[v.j];
   const float s = __ldg(pb.sens + (size_t)__ldg(&v.item->subset) * pb.nvox + v.j);
   const float q = ((double)b > kEps && (double)s > kEps) ? __fdiv_rn(b, s) : 0.0f;
   const float x0 = pb.img[v.j];
   float x = ((double)x0 > kEps && (double)q > kEps) ? __fmul_rn(x0, q) : 0.0f;
   pb.bp[v.j] = 0.0f;
+  if (jt >= 0)
+  {
+    pb.bp_t[jt] = 0.0f;
+  }
   if (!__ldg(&v.item->filter))
   {
     if (pb.cut > 0.0f && radius_at(pb, v.j) > (double)pb.cut)
@@ -154,6 +175,10 @@ __global__ void __launch_bounds__(kBatchBlock) k_batch_em(const BatchProblem* __
       x = 0.0f;
     }
     pb.wide[v.j] = (double)x;
+    if (jt >= 0)
+    {
+      pb.wide_t[jt] = (double)x;
+    }
   }
   pb.img[v.j] = x;
 }
@@ -223,6 +248,10 @@ __global__ void __launch_bounds__(kBatchBlock) k_batch_filter(const BatchProblem
     }
     pb.img[j] = x;
     pb.wide[j] = (double)x;
+    if (pb.wide_t != nullptr)
+    {
+      pb.wide_t[exchanged(pb, j)] = (double)x;
+    }
   }
 }
 }  // namespace

@@ -32,9 +32,10 @@ struct fir_batch
     int n_sub_total = 0;
     int n_enum = 0;
     bool filter = false;
+    bool exchanged = false;  // x/y-exchanged images for LORs along x (use_exchanged)
     double path = 0.0;  // nx + ny + nz: relative cost of a bundle
-    size_t off_sino = 0, off_sens = 0, off_img = 0, off_wide = 0, off_bp = 0, off_t1 = 0, off_t2 = 0,
-           off_xy = 0, off_z = 0;
+    size_t off_sino = 0, off_sens = 0, off_img = 0, off_wide = 0, off_bp = 0, off_wide_t = 0, off_bp_t = 0,
+           off_t1 = 0, off_t2 = 0, off_xy = 0, off_z = 0;
     DevBuf bias;
   };
   struct Launch
@@ -269,6 +270,9 @@ fir_status fir_batch_create(fir_batch** out, fir_ctx* ctx, int n_problems, const
       q.off_img = take(nv * sizeof(float));
       q.off_wide = take(nv * sizeof(double));
       q.off_bp = take(nv * sizeof(float));
+      q.exchanged = use_exchanged(c, grid_of(c, q.v));
+      q.off_wide_t = take(q.exchanged ? nv * sizeof(double) : 0);
+      q.off_bp_t = take(q.exchanged ? nv * sizeof(float) : 0);
       q.off_t1 = take(q.filter ? nv * sizeof(float) : 0);
       q.off_t2 = take(q.filter ? nv * sizeof(float) : 0);
       q.off_xy = take(scan[(size_t)k].xy.size() * sizeof(double));
@@ -302,6 +306,8 @@ fir_status fir_batch_create(fir_batch** out, fir_ctx* ctx, int n_problems, const
         d.img = reinterpret_cast<float*>(base + q.off_img);
         d.wide = reinterpret_cast<double*>(base + q.off_wide);
         d.bp = reinterpret_cast<float*>(base + q.off_bp);
+        d.wide_t = q.exchanged ? reinterpret_cast<double*>(base + q.off_wide_t) : nullptr;
+        d.bp_t = q.exchanged ? reinterpret_cast<float*>(base + q.off_bp_t) : nullptr;
         d.t1 = q.filter ? reinterpret_cast<float*>(base + q.off_t1) : nullptr;
         d.t2 = q.filter ? reinterpret_cast<float*>(base + q.off_t2) : nullptr;
         d.nvox = (int)q.v.nvox;

@@ -148,6 +148,7 @@ struct fir_ctx
   long long det_chunk = 1LL << 28;
   int step_limit = 0;  // FIR_OPT_STEP_LIMIT
   long long launches = 0;
+  long long l2_bytes = 0;  // the device's L2 size, read on first use
 
   bool have_scanner = false;
   int scan_rings = 0, scan_cpr = 0;
@@ -179,6 +180,10 @@ namespace fir::abi
 fir_ctx& check_ctx(fir_ctx* c);
 // The traversal grid of a volume under the context's geometry mode.
 Grid grid_of(const fir_ctx& c, const VolInfo& v);
+// Whether the fused OSEM kernel uses x/y-exchanged images for LORs running
+// mostly along x: while both orientations of the double image and of the
+// accumulator (24 bytes per voxel) fit in L2.
+bool use_exchanged(fir_ctx& c, const Grid& g);
 // The enumeration of subset `subset` of n_subsets.
 Sino sino_of(const ProjInfo& p, int n_subsets, int subset);
 // Reads and clears the device check word; fails when it is set.

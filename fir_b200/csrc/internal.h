@@ -124,6 +124,8 @@ struct BatchProblem
   float* img;
   double* wide;  // double copy of img for the projector gathers
   float* bp;
+  double* wide_t;  // wide and bp with x and y exchanged ([z][x][y]), for LORs
+  float* bp_t;     // running mostly along x; bp_t is added into bp by the EM step
   float* t1;
   float* t2;
   int nvox;

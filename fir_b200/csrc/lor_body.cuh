@@ -102,10 +102,10 @@ __device__ __forceinline__ void osem_lor_body(const Grid& g, const Sino& s, int 
 }
 // FIR's sub-iteration body (reconAlgos.cc:119-158).
 __device__ __forceinline__ void osem_lor(const Grid& g, const Sino& s, int subset, const Tables& t,
-                                         const double* __restrict__ img, const float* __restrict__ sino,
-                                         const float* __restrict__ bias, float* bp, bool skip_zero, int i,
-                                         int* check)
+                                         const double* __restrict__ img, const double* __restrict__ img_t,
+                                         const float* __restrict__ sino, const float* __restrict__ bias, float* bp,
+                                         float* bp_t, bool skip_zero, int i, int* check)
 {
-  osem_lor_body<false>(g, s, subset, t, img, nullptr, sino, nullptr, bias, bp, nullptr, skip_zero, i, check);
+  osem_lor_body<false>(g, s, subset, t, img, img_t, sino, nullptr, bias, bp, bp_t, skip_zero, i, check);
 }
 }  // namespace fir
