@@ -538,7 +538,7 @@ Tables tables_of(fir_ctx& c, const ProjInfo& p)
 // touch, but double the image bytes in use.  With both orientations in L2
 // they pay (clinical 200x200x64 volume: subset kernel 2.36 -> 2.09 ms); a
 // 320x320x128 volume (315 MB for both) ran 4 % slower with them.
-bool use_exchanged(fir_ctx& c, const Grid& g)
+bool use_exchanged(fir_ctx& c, const Grid& g, double bytes_per_voxel)
 {
   if ((g.ny + 31) / 32 > 65535)
   {
@@ -550,7 +550,7 @@ bool use_exchanged(fir_ctx& c, const Grid& g)
     cuda_ok(cudaDeviceGetAttribute(&v, cudaDevAttrL2CacheSize, c.device), "cudaDeviceGetAttribute");
     c.l2_bytes = v > 0 ? v : 1;
   }
-  return 24.0 * g.nx * g.ny * g.nz <= (double)c.l2_bytes;
+  return bytes_per_voxel * g.nx * g.ny * g.nz <= (double)c.l2_bytes;
 }
 
 Grid grid_of(const fir_ctx& c, const VolInfo& v)
@@ -1474,11 +1474,16 @@ fir_status fir_forward_frames(fir_ctx* ctx, const fir_vol_desc* vol, const void*
     for (int f0 = 0; f0 < nfr; f0 += kMaxFramesPerPass)
     {
       const int nf = std::min(kMaxFramesPerPass, nfr - f0);
-      auto* il = static_cast<double*>(c.frames_il.ensure((size_t)v.nvox * frames_stride(nf) * sizeof(double)));
-      launch_interleave(v.nvox, nf, dimg + (size_t)f0 * v.nvox * es, f64, il, cfg_of(c));
+      const size_t il_bytes = (size_t)v.nvox * frames_stride(nf) * sizeof(double);
+      auto* il = static_cast<double*>(c.frames_il.ensure(il_bytes));
+      auto* il_t = use_exchanged(c, g, 2.0 * frames_stride(nf) * sizeof(double))
+                       ? static_cast<double*>(c.frames_il_t.ensure(il_bytes))
+                       : nullptr;
+      launch_interleave(v.nvox, nf, g.nx, g.ny, dimg + (size_t)f0 * v.nvox * es, f64, il, il_t, cfg_of(c));
       after_launch(c);
       timed_launch(c, [&] {
-        launch_forward_frames(g, s, t, il, nf, p.g.n_bins, dsino + (size_t)f0 * p.g.n_bins * es, f64, cfg_of(c));
+        launch_forward_frames(g, s, t, il, il_t, nf, p.g.n_bins, dsino + (size_t)f0 * p.g.n_bins * es, f64,
+                              cfg_of(c));
       });
     }
     finish(c, st);
@@ -1511,11 +1516,17 @@ fir_status fir_backward_frames(fir_ctx* ctx, const fir_proj_desc* proj, const vo
       const size_t acc_bytes = (size_t)v.nvox * frames_stride(nf) * es;
       void* acc = c.frames_acc.ensure(acc_bytes);
       cuda_ok(cudaMemsetAsync(acc, 0, acc_bytes, c.stream), "cudaMemsetAsync");
+      void* acc_t = nullptr;
+      if (use_exchanged(c, g, 2.0 * frames_stride(nf) * es))
+      {
+        acc_t = c.frames_acc_t.ensure(acc_bytes);
+        cuda_ok(cudaMemsetAsync(acc_t, 0, acc_bytes, c.stream), "cudaMemsetAsync");
+      }
       timed_launch(c, [&] {
-        launch_backward_frames(g, s, t, dsino + (size_t)f0 * p.g.n_bins * es, nf, p.g.n_bins, acc, f64,
+        launch_backward_frames(g, s, t, dsino + (size_t)f0 * p.g.n_bins * es, nf, p.g.n_bins, acc, acc_t, f64,
                                c.skip_zero != 0, cfg_of(c));
       });
-      launch_deinterleave(v.nvox, nf, acc, f64, dimg + (size_t)f0 * v.nvox * es, cfg_of(c));
+      launch_deinterleave(v.nvox, nf, g.nx, g.ny, acc, acc_t, f64, dimg + (size_t)f0 * v.nvox * es, cfg_of(c));
       after_launch(c);
     }
     finish(c, st);

@@ -159,6 +159,7 @@ struct fir_ctx
 
   fir::abi::DevBuf bp, conv1, conv2, conv_copy, mu, wide, det, det_pairs, ratio, frames_il, frames_acc, psf_blur, psf_sens, rebin;
   fir::abi::DevBuf wide_t, bp_t;  // x/y-exchanged double image and accumulator of the fused kernel
+  fir::abi::DevBuf frames_il_t, frames_acc_t;  // the same for the multi-frame projectors
   std::vector<fir::abi::DevBuf> staging;
 
   // pipelined input of fir_osem from pinned host memory
@@ -180,10 +181,11 @@ namespace fir::abi
 fir_ctx& check_ctx(fir_ctx* c);
 // The traversal grid of a volume under the context's geometry mode.
 Grid grid_of(const fir_ctx& c, const VolInfo& v);
-// Whether the fused OSEM kernel uses x/y-exchanged images for LORs running
-// mostly along x: while both orientations of the double image and of the
-// accumulator (24 bytes per voxel) fit in L2.
-bool use_exchanged(fir_ctx& c, const Grid& g);
+// Whether a projector uses x/y-exchanged images for LORs running mostly
+// along x: while both orientations of the images it reads and accumulates
+// (bytes_per_voxel, both orientations counted; 24 for the fused OSEM
+// kernel's double image and float accumulator) fit in L2.
+bool use_exchanged(fir_ctx& c, const Grid& g, double bytes_per_voxel = 24.0);
 // The enumeration of subset `subset` of n_subsets.
 Sino sino_of(const ProjInfo& p, int n_subsets, int subset);
 // Reads and clears the device check word; fails when it is set.

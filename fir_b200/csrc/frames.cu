@@ -36,20 +36,24 @@ __device__ __forceinline__ void red_add_v2(float* p, float a, float b)
 
 template<int FMAX, bool F64>
 __global__ void __launch_bounds__(256, 4) k_forward_frames(Grid g, Sino s, Tables t, const double* __restrict__ il,
-                                                        int nf, long long n_bins, void* out, int* check)
+                                                        const double* __restrict__ il_t, int nf, long long n_bins,
+                                                        void* out, int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < s.n_enum;
   Lor l{};
   Walk w{};
   bool go = false;
+  bool tr = false;
   if (valid)
   {
     l = decode_bin(s, i);
     double e[6];
     lor_ends(s, t, l, e);
-    go = siddon_setup(g, e, w);
+    tr = il_t != nullptr && fabs(dsub(e[3], e[0])) > fabs(dsub(e[4], e[1]));
+    go = siddon_setup(g, e, w, tr);
   }
+  const double* src = tr ? il_t : il;
   float lf[FMAX];
   double ld[FMAX];
 #pragma unroll
@@ -64,12 +68,12 @@ __global__ void __launch_bounds__(256, 4) k_forward_frames(Grid g, Sino s, Table
       double x[FMAX];
       if (FMAX == 1)
       {
-        x[0] = __ldg(il + c);
+        x[0] = __ldg(src + c);
       }
       else
       {
         // a voxel's frames are 16-byte aligned: FMAX doubles at c * FMAX
-        const double2* v = reinterpret_cast<const double2*>(il + (size_t)c * FMAX);
+        const double2* v = reinterpret_cast<const double2*>(src + (size_t)c * FMAX);
 #pragma unroll
         for (int k = 0; k < FMAX / 2; ++k)
         {
@@ -113,12 +117,13 @@ __global__ void __launch_bounds__(256, 4) k_forward_frames(Grid g, Sino s, Table
 
 template<int FMAX, bool F64>
 __global__ void __launch_bounds__(256, 4) k_backward_frames(Grid g, Sino s, Tables t, const void* __restrict__ sino,
-                                                         int nf, long long n_bins, void* acc, int skip_zero,
-                                                         int* check)
+                                                         int nf, long long n_bins, void* acc_n, void* acc_t,
+                                                         int skip_zero, int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   Walk w{};
   bool go = false;
+  bool tr = false;
   double v[FMAX];
 #pragma unroll
   for (int f = 0; f < FMAX; ++f)
@@ -144,9 +149,11 @@ __global__ void __launch_bounds__(256, 4) k_backward_frames(Grid g, Sino s, Tabl
     {
       double e[6];
       lor_ends(s, t, l, e);
-      go = siddon_setup(g, e, w);
+      tr = acc_t != nullptr && fabs(dsub(e[3], e[0])) > fabs(dsub(e[4], e[1]));
+      go = siddon_setup(g, e, w, tr);
     }
   }
+  void* acc = tr ? acc_t : acc_n;
   const bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
     if (inside)
     {
@@ -197,9 +204,24 @@ __global__ void __launch_bounds__(256, 4) k_backward_frames(Grid g, Sino s, Tabl
   }
 }
 
-// il[j * fmax + f] = frame f of img at voxel j (widened), 0 for f >= nf.
+// Index of voxel j in the layout with x and y exchanged ([z][x][y]).
+__device__ __forceinline__ long long exchanged(long long j, int nx, int ny)
+{
+  const long long r = j / nx;
+  const int x = (int)(j - r * nx);
+  const long long z = r / ny;
+  const int y = (int)(r - z * ny);
+  return (z * nx + x) * ny + y;
+}
+
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+
+// il[j * fmax + f] = frame f of img at voxel j (widened), 0 for f >= nf;
+// il_t (when given) the same with x and y exchanged.
 template<typename T>
-__global__ void k_interleave(long long nvox, int nf, int fmax, const T* __restrict__ img, double* __restrict__ il)
+__global__ void k_interleave(long long nvox, int nf, int fmax, int nx, int ny, const T* __restrict__ img,
+                             double* __restrict__ il, double* __restrict__ il_t)
 {
   const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (k >= nvox * fmax)
@@ -208,12 +230,19 @@ __global__ void k_interleave(long long nvox, int nf, int fmax, const T* __restri
   }
   const long long j = k / fmax;
   const int f = (int)(k - j * fmax);
-  il[k] = f < nf ? (double)img[(size_t)f * nvox + j] : 0.0;
+  const double v = f < nf ? (double)img[(size_t)f * nvox + j] : 0.0;
+  il[k] = v;
+  if (il_t != nullptr)
+  {
+    il_t[exchanged(j, nx, ny) * fmax + f] = v;
+  }
 }
 
-// img[f][j] = acc[j * fmax + f] for f < nf.
+// img[f][j] = acc[j * fmax + f] (+ the exchanged accumulator's value) for
+// f < nf.
 template<typename T>
-__global__ void k_deinterleave(long long nvox, int nf, int fmax, const T* __restrict__ acc, T* __restrict__ img)
+__global__ void k_deinterleave(long long nvox, int nf, int fmax, int nx, int ny, const T* __restrict__ acc,
+                               const T* __restrict__ acc_t, T* __restrict__ img)
 {
   const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (k >= nvox * nf)
@@ -222,7 +251,8 @@ __global__ void k_deinterleave(long long nvox, int nf, int fmax, const T* __rest
   }
   const int f = (int)(k / nvox);
   const long long j = k - (long long)f * nvox;
-  img[k] = acc[j * fmax + f];
+  const T a = acc[j * fmax + f];
+  img[k] = acc_t != nullptr ? add_rn(a, acc_t[exchanged(j, nx, ny) * fmax + f]) : a;
 }
 
 unsigned blocks_for(long long n, int block)
@@ -231,26 +261,26 @@ unsigned blocks_for(long long n, int block)
 }
 
 template<int FMAX>
-void fwd(const Grid& g, const Sino& s, const Tables& t, const double* il, int nf, long long n_bins, void* out,
-         bool f64, const LaunchCfg& cfg)
+void fwd(const Grid& g, const Sino& s, const Tables& t, const double* il, const double* il_t, int nf,
+         long long n_bins, void* out, bool f64, const LaunchCfg& cfg)
 {
   const unsigned nb = blocks_for(s.n_enum, cfg.block);
   if (f64)
-    k_forward_frames<FMAX, true><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, il, nf, n_bins, out, cfg.check);
+    k_forward_frames<FMAX, true><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, il, il_t, nf, n_bins, out, cfg.check);
   else
-    k_forward_frames<FMAX, false><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, il, nf, n_bins, out, cfg.check);
+    k_forward_frames<FMAX, false><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, il, il_t, nf, n_bins, out, cfg.check);
 }
 
 template<int FMAX>
 void bwd(const Grid& g, const Sino& s, const Tables& t, const void* sino, int nf, long long n_bins, void* acc,
-         bool f64, bool skip_zero, const LaunchCfg& cfg)
+         void* acc_t, bool f64, bool skip_zero, const LaunchCfg& cfg)
 {
   const unsigned nb = blocks_for(s.n_enum, cfg.block);
   if (f64)
-    k_backward_frames<FMAX, true><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, sino, nf, n_bins, acc,
+    k_backward_frames<FMAX, true><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, sino, nf, n_bins, acc, acc_t,
                                                                      skip_zero ? 1 : 0, cfg.check);
   else
-    k_backward_frames<FMAX, false><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, sino, nf, n_bins, acc,
+    k_backward_frames<FMAX, false><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, sino, nf, n_bins, acc, acc_t,
                                                                       skip_zero ? 1 : 0, cfg.check);
 }
 }  // namespace
@@ -260,30 +290,33 @@ int frames_stride(int nf)
   return nf <= 1 ? 1 : (nf <= 2 ? 2 : kMaxFramesPerPass);
 }
 
-void launch_interleave(long long nvox, int nf, const void* img, bool f64, double* il, const LaunchCfg& cfg)
+void launch_interleave(long long nvox, int nf, int nx, int ny, const void* img, bool f64, double* il, double* il_t,
+                       const LaunchCfg& cfg)
 {
   const int fmax = frames_stride(nf);
   const unsigned nb = blocks_for(nvox * fmax, 256);
   if (f64)
-    k_interleave<double><<<nb, 256, 0, cfg.stream>>>(nvox, nf, fmax, static_cast<const double*>(img), il);
+    k_interleave<double><<<nb, 256, 0, cfg.stream>>>(nvox, nf, fmax, nx, ny, static_cast<const double*>(img), il,
+                                                     il_t);
   else
-    k_interleave<float><<<nb, 256, 0, cfg.stream>>>(nvox, nf, fmax, static_cast<const float*>(img), il);
+    k_interleave<float><<<nb, 256, 0, cfg.stream>>>(nvox, nf, fmax, nx, ny, static_cast<const float*>(img), il, il_t);
 }
 
-void launch_deinterleave(long long nvox, int nf, const void* acc, bool f64, void* img, const LaunchCfg& cfg)
+void launch_deinterleave(long long nvox, int nf, int nx, int ny, const void* acc, const void* acc_t, bool f64,
+                         void* img, const LaunchCfg& cfg)
 {
   const int fmax = frames_stride(nf);
   const unsigned nb = blocks_for(nvox * nf, 256);
   if (f64)
-    k_deinterleave<double><<<nb, 256, 0, cfg.stream>>>(nvox, nf, fmax, static_cast<const double*>(acc),
-                                                       static_cast<double*>(img));
+    k_deinterleave<double><<<nb, 256, 0, cfg.stream>>>(nvox, nf, fmax, nx, ny, static_cast<const double*>(acc),
+                                                       static_cast<const double*>(acc_t), static_cast<double*>(img));
   else
-    k_deinterleave<float><<<nb, 256, 0, cfg.stream>>>(nvox, nf, fmax, static_cast<const float*>(acc),
-                                                      static_cast<float*>(img));
+    k_deinterleave<float><<<nb, 256, 0, cfg.stream>>>(nvox, nf, fmax, nx, ny, static_cast<const float*>(acc),
+                                                      static_cast<const float*>(acc_t), static_cast<float*>(img));
 }
 
-void launch_forward_frames(const Grid& g, const Sino& s, const Tables& t, const double* il, int nf, long long n_bins,
-                           void* out, bool f64, const LaunchCfg& cfg)
+void launch_forward_frames(const Grid& g, const Sino& s, const Tables& t, const double* il, const double* il_t, int nf,
+                           long long n_bins, void* out, bool f64, const LaunchCfg& cfg)
 {
   if (s.n_enum == 0 || nf <= 0)
   {
@@ -291,14 +324,14 @@ void launch_forward_frames(const Grid& g, const Sino& s, const Tables& t, const 
   }
   switch (frames_stride(nf))
   {
-    case 1: fwd<1>(g, s, t, il, nf, n_bins, out, f64, cfg); break;
-    case 2: fwd<2>(g, s, t, il, nf, n_bins, out, f64, cfg); break;
-    default: fwd<kMaxFramesPerPass>(g, s, t, il, nf, n_bins, out, f64, cfg); break;
+    case 1: fwd<1>(g, s, t, il, il_t, nf, n_bins, out, f64, cfg); break;
+    case 2: fwd<2>(g, s, t, il, il_t, nf, n_bins, out, f64, cfg); break;
+    default: fwd<kMaxFramesPerPass>(g, s, t, il, il_t, nf, n_bins, out, f64, cfg); break;
   }
 }
 
 void launch_backward_frames(const Grid& g, const Sino& s, const Tables& t, const void* sino, int nf,
-                            long long n_bins, void* acc, bool f64, bool skip_zero, const LaunchCfg& cfg)
+                            long long n_bins, void* acc, void* acc_t, bool f64, bool skip_zero, const LaunchCfg& cfg)
 {
   if (s.n_enum == 0 || nf <= 0)
   {
@@ -306,9 +339,9 @@ void launch_backward_frames(const Grid& g, const Sino& s, const Tables& t, const
   }
   switch (frames_stride(nf))
   {
-    case 1: bwd<1>(g, s, t, sino, nf, n_bins, acc, f64, skip_zero, cfg); break;
-    case 2: bwd<2>(g, s, t, sino, nf, n_bins, acc, f64, skip_zero, cfg); break;
-    default: bwd<kMaxFramesPerPass>(g, s, t, sino, nf, n_bins, acc, f64, skip_zero, cfg); break;
+    case 1: bwd<1>(g, s, t, sino, nf, n_bins, acc, acc_t, f64, skip_zero, cfg); break;
+    case 2: bwd<2>(g, s, t, sino, nf, n_bins, acc, acc_t, f64, skip_zero, cfg); break;
+    default: bwd<kMaxFramesPerPass>(g, s, t, sino, nf, n_bins, acc, acc_t, f64, skip_zero, cfg); break;
   }
 }
 }  // namespace fir

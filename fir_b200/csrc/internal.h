@@ -180,14 +180,20 @@ int batch_max_resident(int block);
 constexpr int kMaxFramesPerPass = 4;
 // Interleave stride of a group of nf frames: 1, 2, 4 or 8.
 int frames_stride(int nf);
-// il[j * stride + f] = (double) frame f of img (float or double, frame-major).
-void launch_interleave(long long nvox, int nf, const void* img, bool f64, double* il, const LaunchCfg& cfg);
-// img[f][j] = acc[j * stride + f] (float or double).
-void launch_deinterleave(long long nvox, int nf, const void* acc, bool f64, void* img, const LaunchCfg& cfg);
+// il[j * stride + f] = (double) frame f of img (float or double, frame-major);
+// il_t (or null) the same with x and y exchanged.
+void launch_interleave(long long nvox, int nf, int nx, int ny, const void* img, bool f64, double* il, double* il_t,
+                       const LaunchCfg& cfg);
+// img[f][j] = acc[j * stride + f] (+ acc_t at the exchanged index when
+// given; float or double).
+void launch_deinterleave(long long nvox, int nf, int nx, int ny, const void* acc, const void* acc_t, bool f64,
+                         void* img, const LaunchCfg& cfg);
 // out[f * n_bins + bin] = projection of frame f (float or double sinograms).
-void launch_forward_frames(const Grid& g, const Sino& s, const Tables& t, const double* il, int nf, long long n_bins,
-                           void* out, bool f64, const LaunchCfg& cfg);
-// acc[c * stride + f] += backprojection of sino[f * n_bins + ...].
+// LORs running mostly along x gather from il_t when it is given.
+void launch_forward_frames(const Grid& g, const Sino& s, const Tables& t, const double* il, const double* il_t, int nf,
+                           long long n_bins, void* out, bool f64, const LaunchCfg& cfg);
+// acc[c * stride + f] += backprojection of sino[f * n_bins + ...]; LORs
+// running mostly along x add into acc_t (x and y exchanged) when it is given.
 void launch_backward_frames(const Grid& g, const Sino& s, const Tables& t, const void* sino, int nf,
-                            long long n_bins, void* acc, bool f64, bool skip_zero, const LaunchCfg& cfg);
+                            long long n_bins, void* acc, void* acc_t, bool f64, bool skip_zero, const LaunchCfg& cfg);
 }  // namespace fir
