@@ -481,6 +481,49 @@ const double* widen(fir_ctx& c, const float* img, long long n)
   return d;
 }
 
+// Double copies of a float image for a projection: with x and y exchanged
+// too while both fit in L2 (use_exchanged).
+struct Widened
+{
+  const double* img;
+  const double* img_t;  // null: one orientation
+};
+
+Widened widen_for_projection(fir_ctx& c, const Grid& g, const float* img)
+{
+  const long long n = (long long)g.nxy * g.nz;
+  if (!use_exchanged(c, g, 16.0))
+  {
+    return Widened{widen(c, img, n), nullptr};
+  }
+  double* d = static_cast<double*>(c.wide.ensure((size_t)n * sizeof(double)));
+  double* d_t = static_cast<double*>(c.wide_t.ensure((size_t)n * sizeof(double)));
+  launch_widen_oriented(g.nx, g.ny, g.nz, img, d, d_t, cfg_of(c));
+  after_launch(c);
+  return Widened{d, d_t};
+}
+
+// img += backprojection of sino (nullptr: all ones) over the subset of s, in
+// the atomic mode; LORs running mostly along x accumulate in an x/y-exchanged
+// scratch image that is added into img afterwards, while both fit in L2.
+void backproject_subset(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, const float* sino, float* img,
+                        bool skip_zero)
+{
+  float* img_t = nullptr;
+  const long long n = (long long)g.nxy * g.nz;
+  if (use_exchanged(c, g, 8.0))
+  {
+    img_t = static_cast<float*>(c.bp_t.ensure((size_t)n * sizeof(float)));
+    cuda_ok(cudaMemsetAsync(img_t, 0, (size_t)n * sizeof(float), c.stream), "cudaMemsetAsync");
+  }
+  timed_launch(c, [&] { launch_backward(g, s, t, sino, img, img_t, skip_zero, cfg_of(c)); });
+  if (img_t != nullptr)
+  {
+    launch_merge_oriented(g.nx, g.ny, g.nz, img, img_t, cfg_of(c));
+    after_launch(c);
+  }
+}
+
 // bp (zeroed by the caller) += backprojection of sino / (projection of img +
 // bias) over the subset of s: the fused kernel, or in deterministic mode the
 // ratio kernel followed by the ordered scatter.  The fused kernel reads and
@@ -1382,8 +1425,8 @@ fir_status fir_forward(fir_ctx* ctx, const fir_vol_desc* vol, const float* img, 
     const float* dimg = st.in(img, v.nvox);
     float* dsino = st.out(sino, p.g.n_bins);
     const Sino s = sino_of(p, 1, 0);
-    const double* wimg = widen(c, dimg, v.nvox);
-    timed_launch(c, [&] { launch_forward(g, s, t, wimg, dsino, FwdEpilogue::None, cfg_of(c)); });
+    const Widened w = widen_for_projection(c, g, dimg);
+    timed_launch(c, [&] { launch_forward(g, s, t, w.img, w.img_t, dsino, FwdEpilogue::None, cfg_of(c)); });
     finish(c, st);
   });
 }
@@ -1401,8 +1444,8 @@ fir_status fir_forward_exp(fir_ctx* ctx, const fir_vol_desc* vol, const float* m
     const float* dmu = st.in(mu, v.nvox);
     float* dacf = st.out(acf, p.g.n_bins);
     const Sino s = sino_of(p, 1, 0);
-    const double* wmu = widen(c, dmu, v.nvox);
-    timed_launch(c, [&] { launch_forward(g, s, t, wmu, dacf, FwdEpilogue::Exp, cfg_of(c)); });
+    const Widened w = widen_for_projection(c, g, dmu);
+    timed_launch(c, [&] { launch_forward(g, s, t, w.img, w.img_t, dacf, FwdEpilogue::Exp, cfg_of(c)); });
     finish(c, st);
   });
 }
@@ -1434,9 +1477,7 @@ fir_status fir_backward(fir_ctx* ctx, const fir_proj_desc* proj, const float* si
         det_backproject(c, g, ss, t, dsino, false, dimg + (size_t)s * v.nvox, v.nvox);
         continue;
       }
-      timed_launch(c, [&] {
-        launch_backward(g, ss, t, dsino, dimg + (size_t)s * v.nvox, c.skip_zero != 0, cfg_of(c));
-      });
+      backproject_subset(c, g, ss, t, dsino, dimg + (size_t)s * v.nvox, c.skip_zero != 0);
     }
     finish(c, st);
   });
@@ -1555,7 +1596,7 @@ fir_status fir_sensitivity(fir_ctx* ctx, const fir_proj_desc* proj, const fir_vo
         det_backproject(c, g, ss, t, nullptr, false, dsens + (size_t)s * v.nvox, v.nvox);
         continue;
       }
-      timed_launch(c, [&] { launch_backward(g, ss, t, nullptr, dsens + (size_t)s * v.nvox, false, cfg_of(c)); });
+      backproject_subset(c, g, ss, t, nullptr, dsens + (size_t)s * v.nvox, false);
     }
     finish(c, st);
   });

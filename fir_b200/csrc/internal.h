@@ -30,9 +30,11 @@ struct LaunchCfg
 };
 
 // projector.cu
-void launch_forward(const Grid& g, const Sino& s, const Tables& t, const double* img, float* sino,
-                    FwdEpilogue ep, const LaunchCfg& cfg);
-void launch_backward(const Grid& g, const Sino& s, const Tables& t, const float* sino, float* img,
+// img_t (or null): the image with x and y exchanged ([z][x][y]), which LORs
+// running mostly along x use; the caller adds a backprojected img_t into img.
+void launch_forward(const Grid& g, const Sino& s, const Tables& t, const double* img, const double* img_t,
+                    float* sino, FwdEpilogue ep, const LaunchCfg& cfg);
+void launch_backward(const Grid& g, const Sino& s, const Tables& t, const float* sino, float* img, float* img_t,
                      bool skip_zero, const LaunchCfg& cfg);
 // mult: per-bin multiplicative factors of the ordinary-Poisson model, or
 // nullptr for FIR's model.

@@ -21,9 +21,12 @@ namespace
 // projections::forward (projections.cc:15-92) with
 // VolData::computeLineIntegral (VolData.cc:357-371); optional epilogue
 // ProjData::exponential (ProjData.cc:514-539).
+// LORs running mostly along x gather from img_t (x and y exchanged) when
+// it is given.
 template<FwdEpilogue EP>
 __global__ void __launch_bounds__(256, 4) k_forward(Grid g, Sino s, Tables t,
                                                  const double* __restrict__ img,
+                                                 const double* __restrict__ img_t,
                                                  float* __restrict__ sino, int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -31,18 +34,21 @@ __global__ void __launch_bounds__(256, 4) k_forward(Grid g, Sino s, Tables t,
   Lor l{};
   Walk w{};
   bool go = false;
+  bool tr = false;
   if (valid)
   {
     l = decode_bin(s, i);
     double e[6];
     lor_ends(s, t, l, e);
-    go = siddon_setup(g, e, w);
+    tr = img_t != nullptr && fabs(dsub(e[3], e[0])) > fabs(dsub(e[4], e[1]));
+    go = siddon_setup(g, e, w, tr);
   }
+  const double* im = tr ? img_t : img;
   float line = 0.0f;
   const bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
     if (inside)
     {
-      line = accumulate(line, len, __ldg(img + c));
+      line = accumulate(line, len, __ldg(im + c));
     }
   });
   if (!ok)
@@ -64,13 +70,16 @@ __global__ void __launch_bounds__(256, 4) k_forward(Grid g, Sino s, Tables t,
 // projections::backward (projections.cc:94-184) with
 // VolData::projectLineIntegral (VolData.cc:373-385).  sino == nullptr is the
 // all-ones sinogram of computeSensitivityVol (projections.cc:186-197).
+// LORs running mostly along x add into img_t (x and y exchanged) when it is
+// given.
 __global__ void __launch_bounds__(256) k_backward(Grid g, Sino s, Tables t,
-                                                  const float* __restrict__ sino, float* img,
+                                                  const float* __restrict__ sino, float* img, float* img_t,
                                                   int skip_zero, int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   Walk w{};
   bool go = false;
+  bool tr = false;
   double v = 0.0;
   if (i < s.n_enum)
   {
@@ -82,13 +91,15 @@ __global__ void __launch_bounds__(256) k_backward(Grid g, Sino s, Tables t,
     {
       double e[6];
       lor_ends(s, t, l, e);
-      go = siddon_setup(g, e, w);
+      tr = img_t != nullptr && fabs(dsub(e[3], e[0])) > fabs(dsub(e[4], e[1]));
+      go = siddon_setup(g, e, w, tr);
     }
   }
+  float* acc = tr ? img_t : img;
   const bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
     if (inside)
     {
-      atomicAdd(img + c, __double2float_rn(dmul(len, v)));
+      atomicAdd(acc + c, __double2float_rn(dmul(len, v)));
     }
   });
   if (!ok)
@@ -191,8 +202,8 @@ unsigned blocks_for(long long n, int block)
 }
 }  // namespace
 
-void launch_forward(const Grid& g, const Sino& s, const Tables& t, const double* img, float* sino,
-                    FwdEpilogue ep, const LaunchCfg& cfg)
+void launch_forward(const Grid& g, const Sino& s, const Tables& t, const double* img, const double* img_t,
+                    float* sino, FwdEpilogue ep, const LaunchCfg& cfg)
 {
   if (s.n_enum == 0)
   {
@@ -201,15 +212,15 @@ void launch_forward(const Grid& g, const Sino& s, const Tables& t, const double*
   const unsigned nb = blocks_for(s.n_enum, cfg.block);
   if (ep == FwdEpilogue::Exp)
   {
-    k_forward<FwdEpilogue::Exp><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, sino, cfg.check);
+    k_forward<FwdEpilogue::Exp><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, img_t, sino, cfg.check);
   }
   else
   {
-    k_forward<FwdEpilogue::None><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, sino, cfg.check);
+    k_forward<FwdEpilogue::None><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, img_t, sino, cfg.check);
   }
 }
 
-void launch_backward(const Grid& g, const Sino& s, const Tables& t, const float* sino, float* img,
+void launch_backward(const Grid& g, const Sino& s, const Tables& t, const float* sino, float* img, float* img_t,
                      bool skip_zero, const LaunchCfg& cfg)
 {
   if (s.n_enum == 0)
@@ -217,7 +228,7 @@ void launch_backward(const Grid& g, const Sino& s, const Tables& t, const float*
     return;
   }
   k_backward<<<blocks_for(s.n_enum, cfg.block), cfg.block, 0, cfg.stream>>>(
-    g, s, t, sino, img, skip_zero ? 1 : 0, cfg.check);
+    g, s, t, sino, img, img_t, skip_zero ? 1 : 0, cfg.check);
 }
 
 void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const double* img, const double* img_t,
