@@ -34,6 +34,16 @@ __device__ __forceinline__ void red_add_v2(float* p, float a, float b)
   asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(__cvta_generic_to_global(p)), "f"(a), "f"(b) : "memory");
 }
 
+// Four doubles from a 32-byte aligned global address in one 256-bit load
+// (sm_100): the L1 serves a lane's whole sector in one wavefront, where two
+// 128-bit loads took two.
+__device__ __forceinline__ void ld_v4(const double* p, double* x)
+{
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(x[0]), "=d"(x[1]), "=d"(x[2]), "=d"(x[3])
+      : "l"(__cvta_generic_to_global(p)));
+}
+
 template<int FMAX, bool F64>
 __global__ void __launch_bounds__(256, 4) k_forward_frames(Grid g, Sino s, Tables t, const double* __restrict__ il,
                                                         const double* __restrict__ il_t, int nf, long long n_bins,
@@ -69,6 +79,11 @@ __global__ void __launch_bounds__(256, 4) k_forward_frames(Grid g, Sino s, Table
       if (FMAX == 1)
       {
         x[0] = __ldg(src + c);
+      }
+      else if (FMAX == 4)
+      {
+        // a voxel's 4 frames are one 32-byte sector: one 256-bit load
+        ld_v4(src + (size_t)c * 4, x);
       }
       else
       {
