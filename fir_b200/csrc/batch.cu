@@ -68,6 +68,9 @@ __global__ void __launch_bounds__(256, 4) k_batch_osem(const BatchProblem* __res
       const int i = (k - __ldg(&items[it].unit_begin)) * 32 + lane;
       osem_lor(pb.g, pb.s, subset, pb.t, pb.wide, pb.wide_t, pb.sino, pb.bias, pb.bp, pb.bp_t, pb.skip_zero != 0, i,
                check);
+      // lanes whose paths ended early wait here, so that the warp starts the
+      // next bundle together instead of splitting across two bundles
+      __syncwarp();
     }
     if (!kPersistent)
     {
