@@ -15,6 +15,13 @@
 // Work is chunked over contiguous ranges of LORs; chunks are reduced in
 // order, each run continuing from the voxel's value after the previous
 // chunk, so chunking does not change the order either.
+//
+// Each LOR's pairs fill a multiple of 8 slots: the last group is padded with
+// pairs whose key is one past the last voxel.  The stable sort puts them in
+// one final run, which the reduction skips.  With padded regions a lane
+// stages 8 pairs in shared memory and writes them as whole sectors; the
+// lanes of a warp start together and emit one pair per step, so their groups
+// mostly fill on the same steps.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -55,18 +62,26 @@ __global__ void __launch_bounds__(256) k_count(Grid g, Sino s, Tables t, const f
   }
   if (valid)
   {
-    counts[i] = k;
+    counts[i] = (k + 7) & ~7;
   }
 }
 
+constexpr int kEmitBlock = 128;
+
 // Writes the pairs of enumerated LORs [first, last) at their offsets
-// (offsets relative to the chunk start).
-__global__ void __launch_bounds__(256) k_emit(Grid g, Sino s, Tables t, const float* __restrict__ vals,
-                                              int vals_by_enum, int first, int last,
-                                              const long long* __restrict__ offsets, long long base,
-                                              unsigned* keys, double* prods)
+// (offsets relative to the chunk start, multiples of 8).  Each lane's
+// 8-pair group leaves as two 16-byte key stores and four 16-byte product
+// stores into one 32-byte and one 64-byte aligned span, instead of eight
+// 4-byte and eight 8-byte stores that each touched 32 lines per warp step.
+__global__ void __launch_bounds__(kEmitBlock) k_emit(Grid g, Sino s, Tables t, const float* __restrict__ vals,
+                                                     int vals_by_enum, int first, int last,
+                                                     const long long* __restrict__ offsets, long long base,
+                                                     unsigned sentinel, unsigned* keys, double* prods)
 {
-  const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ unsigned sk[8][kEmitBlock];
+  __shared__ double sp[8][kEmitBlock];
+  const int tid = threadIdx.x;
+  const int i = first + blockIdx.x * kEmitBlock + tid;
   const bool valid = i < last;
   Walk w{};
   bool go = false;
@@ -85,47 +100,72 @@ __global__ void __launch_bounds__(256) k_emit(Grid g, Sino s, Tables t, const fl
       go = siddon_setup(g, e, w);
     }
   }
+  int slot = 0;
+  auto flush = [&]() {
+    uint4* kd = reinterpret_cast<uint4*>(keys + at);
+    kd[0] = make_uint4(sk[0][tid], sk[1][tid], sk[2][tid], sk[3][tid]);
+    kd[1] = make_uint4(sk[4][tid], sk[5][tid], sk[6][tid], sk[7][tid]);
+    double2* pd = reinterpret_cast<double2*>(prods + at);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+    {
+      pd[q] = make_double2(sp[2 * q][tid], sp[2 * q + 1][tid]);
+    }
+    at += 8;
+  };
   siddon_walk(g, w, go, [&](bool inside, int c, double len) {
     if (inside)
     {
-      keys[at] = (unsigned)c;
-      prods[at] = dmul(len, v);
-      ++at;
+      sk[slot][tid] = (unsigned)c;
+      sp[slot][tid] = dmul(len, v);
+      if (++slot == 8)
+      {
+        flush();
+        slot = 0;
+      }
     }
   });
+  if (slot > 0)
+  {
+    for (int q = slot; q < 8; ++q)
+    {
+      sk[q][tid] = sentinel;
+      sp[q][tid] = 0.0;
+    }
+    flush();
+  }
 }
 
-// One warp per run of equal voxel (run r: voxel[r], products [start[r],
-// start[r] + len[r]) of the sorted array): the warp loads 32 products at a
-// time, coalesced, and every lane replays FIR's sequential accumulation
-// float(double(acc) + product) in run order through shuffles, so the lanes
-// stay converged and the order is exactly the run's.
+// One thread per run of equal voxel (run r: voxel[r], products [start[r],
+// start[r] + len[r]) of the sorted array) replays FIR's sequential
+// accumulation float(double(acc) + product) in run order.  Neighbouring
+// threads take neighbouring voxels, whose runs have similar lengths, and each
+// streams its own contiguous run through L1.  (A warp per run, every lane
+// replaying the run through shuffles, spent 32 lanes' worth of conversions
+// per product and was bound by the conversion pipe: 8.4 ms against this.)
 __global__ void __launch_bounds__(256) k_reduce_runs(const int* __restrict__ n_runs, const unsigned* __restrict__ voxel,
                                                      const int* __restrict__ start, const int* __restrict__ len,
-                                                     const double* __restrict__ prods, float* img)
+                                                     const double* __restrict__ prods, unsigned n_vox, float* img)
 {
-  const long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+  const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (r >= *n_runs)
   {
-    return;  // the whole warp: r is the same on every lane
+    return;
   }
   const unsigned v = voxel[r];
-  const int first = start[r], n = len[r];
+  if (v >= n_vox)
+  {
+    return;  // the padding run
+  }
+  const double* p = prods + start[r];
+  const int n = len[r];
   float acc = img[v];
-  for (int base = 0; base < n; base += 32)
+#pragma unroll 4
+  for (int k = 0; k < n; ++k)
   {
-    const int k_end = n - base < 32 ? n - base : 32;
-    const double p = lane < k_end ? prods[first + base + lane] : 0.0;
-    for (int k = 0; k < k_end; ++k)
-    {
-      acc = __double2float_rn(dadd((double)acc, __shfl_sync(0xffffffffu, p, k)));
-    }
+    acc = __double2float_rn(dadd((double)acc, __ldg(p + k)));
   }
-  if (lane == 0)
-  {
-    img[v] = acc;
-  }
+  img[v] = acc;
 }
 
 // The ratio of one OSEM sub-iteration per enumerated LOR
@@ -266,14 +306,15 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
     return cudaGetLastError();
   }
 
-  // 2. pair buffers for chunks of at most max_pairs (at least one LOR's path)
+  // 2. pair buffers for chunks of at most max_pairs (at least one LOR's
+  // padded path)
   long long max_pairs = total < max_pairs_cap ? total : max_pairs_cap;
-  if (max_pairs < g.guard)
+  if (max_pairs < g.guard + 8)
   {
-    max_pairs = g.guard;
+    max_pairs = g.guard + 8;
   }
-  // runs of one chunk: at most one per voxel and one per pair
-  const long long max_runs = max_pairs < n_vox ? max_pairs : n_vox;
+  // runs of one chunk: at most one per voxel, the padding run, and one per pair
+  const long long max_runs = max_pairs < n_vox + 1 ? max_pairs : n_vox + 1;
   size_t sort_bytes = 0, rle_bytes = 0, run_scan_bytes = 0;
   e = cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const unsigned*)nullptr, (unsigned*)nullptr,
                                       (const double*)nullptr, (double*)nullptr, (int)max_pairs, 0, 32, cfg.stream);
@@ -312,7 +353,7 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
   void* sort_tmp = pb + 2 * kslab + 2 * pslab + 3 * rslab + 256;
 
   // 3. chunks of whole LORs, reduced in order
-  const int key_bits = bits_for(n_vox);
+  const int key_bits = bits_for(n_vox + 1);  // the padding key n_vox included
   long long first = 0;
   while (first < n)
   {
@@ -324,8 +365,9 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
     const long long m = off[(size_t)last] - off[(size_t)first];
     if (m > 0)
     {
-      k_emit<<<blocks_for(last - first, cfg.block), cfg.block, 0, cfg.stream>>>(
-        g, s, t, vals, vals_by_enum ? 1 : 0, (int)first, (int)last, offsets, off[(size_t)first], keys_a, prods_a);
+      k_emit<<<blocks_for(last - first, kEmitBlock), kEmitBlock, 0, cfg.stream>>>(
+        g, s, t, vals, vals_by_enum ? 1 : 0, (int)first, (int)last, offsets, off[(size_t)first], (unsigned)n_vox,
+        keys_a, prods_a);
       size_t tmp = tmp_bytes;
       e = cub::DeviceRadixSort::SortPairs(sort_tmp, tmp, keys_a, keys_b, prods_a, prods_b, (int)m, 0, key_bits,
                                           cfg.stream);
@@ -346,8 +388,8 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
       {
         return e;
       }
-      k_reduce_runs<<<blocks_for(runs_cap * 32, 256), 256, 0, cfg.stream>>>(n_runs, run_voxel, run_start, run_len,
-                                                                           prods_b, img);
+      k_reduce_runs<<<blocks_for(runs_cap, 256), 256, 0, cfg.stream>>>(n_runs, run_voxel, run_start, run_len,
+                                                                      prods_b, (unsigned)n_vox, img);
       *launches += 2;
     }
     first = last;
