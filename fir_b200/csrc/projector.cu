@@ -11,7 +11,11 @@
 // stay converged and __syncwarp() between two traversals is safe.  Paths are
 // recomputed on the fly (no LOR cache, no stored path).  The image is
 // gathered from a double-precision copy (exact widening of the float image,
-// made once per call), which stays resident in the 126 MB L2.
+// made once per call), which stays resident in the 126 MB L2.  While both fit
+// in L2, LORs running mostly along x gather from (and backproject into) a
+// copy with x and y exchanged: a warp's parallel LORs are then offset along
+// the contiguous axis in either case, and its accesses touch about half as
+// many cache lines.
 #include "lor_body.cuh"
 
 namespace fir
