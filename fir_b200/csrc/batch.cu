@@ -48,7 +48,10 @@ __device__ __forceinline__ int take(int* queue, int grab, int lane)
   return __shfl_sync(0xffffffffu, v, 0);
 }
 
-template<bool kPersistent>
+// TImg: what the projection gathers from, each problem's double copy or (for
+// problems whose double copy does not fit in L2 beside the accumulator) its
+// float image.  A launch covers problems of one kind.
+template<bool kPersistent, typename TImg>
 __global__ void __launch_bounds__(256, 4) k_batch_osem(const BatchProblem* __restrict__ P,
                                                     const BatchItem* __restrict__ items, int n_items,
                                                     int n_bundles, int* queue, int grab, int* check)
@@ -66,8 +69,16 @@ __global__ void __launch_bounds__(256, 4) k_batch_osem(const BatchProblem* __res
       const int subset = __ldg(&items[it].subset);
       const BatchProblem& pb = P[p];
       const int i = (k - __ldg(&items[it].unit_begin)) * 32 + lane;
-      osem_lor(pb.g, pb.s, subset, pb.t, pb.wide, pb.wide_t, pb.sino, pb.bias, pb.bp, pb.bp_t, pb.skip_zero != 0, i,
-               check);
+      if constexpr (sizeof(TImg) == sizeof(double))
+      {
+        osem_lor(pb.g, pb.s, subset, pb.t, pb.wide, pb.wide_t, pb.sino, pb.bias, pb.bp, pb.bp_t, pb.skip_zero != 0,
+                 i, check);
+      }
+      else
+      {
+        osem_lor_body<false, float>(pb.g, pb.s, subset, pb.t, pb.img, nullptr, pb.sino, nullptr, pb.bias, pb.bp,
+                                    nullptr, pb.skip_zero != 0, i, check);
+      }
       // lanes whose paths ended early wait here, so that the warp starts the
       // next bundle together instead of splitting across two bundles
       __syncwarp();
@@ -138,7 +149,10 @@ __global__ void __launch_bounds__(kBatchBlock) k_batch_prepare(const BatchProble
   {
     pb.img[v.j] = x;
   }
-  pb.wide[v.j] = (double)x;
+  if (pb.wide != nullptr)
+  {
+    pb.wide[v.j] = (double)x;
+  }
   pb.bp[v.j] = 0.0f;
   if (pb.wide_t != nullptr)
   {
@@ -177,7 +191,10 @@ __global__ void __launch_bounds__(kBatchBlock) k_batch_em(const BatchProblem* __
     {
       x = 0.0f;
     }
-    pb.wide[v.j] = (double)x;
+    if (pb.wide != nullptr)
+    {
+      pb.wide[v.j] = (double)x;
+    }
     if (jt >= 0)
     {
       pb.wide_t[jt] = (double)x;
@@ -250,7 +267,10 @@ __global__ void __launch_bounds__(kBatchBlock) k_batch_filter(const BatchProblem
       }
     }
     pb.img[j] = x;
-    pb.wide[j] = (double)x;
+    if (pb.wide != nullptr)
+    {
+      pb.wide[j] = (double)x;
+    }
     if (pb.wide_t != nullptr)
     {
       pb.wide_t[exchanged(pb, j)] = (double)x;
@@ -268,19 +288,18 @@ void launch_batch_prepare(const BatchProblem* P, const BatchItem* items, int n_i
   }
 }
 
-void launch_batch_project(const BatchProblem* P, const BatchItem* items, int n_items, int n_bundles,
-                          int* queue, const BatchLaunch& L, int n_sms, int* check, cudaStream_t stream)
+namespace
 {
-  if (n_bundles <= 0)
-  {
-    return;
-  }
+template<typename TImg>
+void project(const BatchProblem* P, const BatchItem* items, int n_items, int n_bundles, int* queue,
+             const BatchLaunch& L, int n_sms, int* check, cudaStream_t stream)
+{
   const long long threads = (long long)n_bundles * 32;
   const long long plain_blocks = (threads + L.block - 1) / L.block;
   if (L.blocks_per_sm <= 0)
   {
-    k_batch_osem<false><<<(unsigned)plain_blocks, L.block, 0, stream>>>(P, items, n_items, n_bundles, nullptr,
-                                                                         1, check);
+    k_batch_osem<false, TImg><<<(unsigned)plain_blocks, L.block, 0, stream>>>(P, items, n_items, n_bundles,
+                                                                               nullptr, 1, check);
     return;
   }
   long long blocks = (long long)n_sms * L.blocks_per_sm;
@@ -288,8 +307,27 @@ void launch_batch_project(const BatchProblem* P, const BatchItem* items, int n_i
   {
     blocks = plain_blocks;
   }
-  k_batch_osem<true><<<(unsigned)blocks, L.block, 0, stream>>>(P, items, n_items, n_bundles, queue, L.grab,
-                                                                check);
+  k_batch_osem<true, TImg><<<(unsigned)blocks, L.block, 0, stream>>>(P, items, n_items, n_bundles, queue, L.grab,
+                                                                      check);
+}
+}  // namespace
+
+void launch_batch_project(const BatchProblem* P, const BatchItem* items, int n_items, int n_bundles,
+                          int* queue, const BatchLaunch& L, int n_sms, int* check, bool gather_float,
+                          cudaStream_t stream)
+{
+  if (n_bundles <= 0)
+  {
+    return;
+  }
+  if (gather_float)
+  {
+    project<float>(P, items, n_items, n_bundles, queue, L, n_sms, check, stream);
+  }
+  else
+  {
+    project<double>(P, items, n_items, n_bundles, queue, L, n_sms, check, stream);
+  }
 }
 
 void launch_batch_em(const BatchProblem* P, const BatchItem* items, int n_items, int n_units, cudaStream_t stream)
@@ -324,7 +362,7 @@ void launch_batch_filter(const BatchProblem* P, const BatchItem* items, int n_it
 int batch_max_resident(int block)
 {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_osem<true>, block, 0) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_osem<true, double>, block, 0) != cudaSuccess)
   {
     cudaGetLastError();
     return 1;

@@ -543,6 +543,15 @@ void ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t
   }
   if (!use_exchanged(c, g))
   {
+    if (!use_exchanged(c, g, 12.0) && use_exchanged(c, g, 8.0))
+    {
+      // the double copy and the accumulator (12 B/voxel) overflow L2, the
+      // float image and the accumulator (8 B/voxel) fit: gather floats
+      timed_launch(c, [&] {
+        launch_osem_subset_float_image(g, s, t, img, sino, mult, bias, bp, c.skip_zero != 0, cfg_of(c));
+      });
+      return;
+    }
     const double* wimg = widen(c, img, nvox);
     timed_launch(c, [&] {
       launch_osem_subset(g, s, t, wimg, nullptr, sino, mult, bias, bp, nullptr, c.skip_zero != 0, cfg_of(c));

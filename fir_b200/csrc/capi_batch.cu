@@ -33,6 +33,7 @@ struct fir_batch
     int n_enum = 0;
     bool filter = false;
     bool exchanged = false;  // x/y-exchanged images for LORs along x (use_exchanged)
+    bool gather_float = false;  // no double copy: too large for L2 beside the accumulator
     double path = 0.0;  // nx + ny + nz: relative cost of a bundle
     size_t off_sino = 0, off_sens = 0, off_img = 0, off_wide = 0, off_bp = 0, off_wide_t = 0, off_bp_t = 0,
            off_t1 = 0, off_t2 = 0, off_xy = 0, off_z = 0;
@@ -44,7 +45,7 @@ struct fir_batch
   };
   struct Step
   {
-    Launch proj, em, filt;
+    Launch proj, proj_f, em, filt;  // proj_f: problems that gather their float images
   };
 
   fir_ctx* ctx = nullptr;
@@ -152,12 +153,14 @@ void check_launch(cudaStream_t s)
   cuda_ok(cudaGetLastError(), "kernel launch");
 }
 
-// Enqueues the projector of one step (queue: that step's zeroed counter).
-void batch_project(fir_batch& b, const fir_batch::Launch& L, int* queue, const BatchLaunch& shape, cudaStream_t s)
+// Enqueues one projector launch of a step (queue: its zeroed counter).
+void batch_project(fir_batch& b, const fir_batch::Launch& L, int* queue, const BatchLaunch& shape, bool gather_float,
+                   cudaStream_t s)
 {
   const auto* P = static_cast<const BatchProblem*>(b.desc.p);
   const auto* I = static_cast<const BatchItem*>(b.items.p) + L.item_off;
-  launch_batch_project(P, I, L.n_items, L.n_units, queue, shape, b.n_sms, static_cast<int*>(b.ctx->check.p), s);
+  launch_batch_project(P, I, L.n_items, L.n_units, queue, shape, b.n_sms, static_cast<int*>(b.ctx->check.p),
+                       gather_float, s);
   check_launch(s);
 }
 
@@ -168,17 +171,23 @@ long long batch_enqueue(fir_batch& b, cudaStream_t s)
   const auto* I = static_cast<const BatchItem*>(b.items.p);
   int* queue = static_cast<int*>(b.queue.p);
   long long n = 0;
-  cuda_ok(cudaMemsetAsync(queue, 0, b.steps.size() * sizeof(int), s), "cudaMemsetAsync");
+  cuda_ok(cudaMemsetAsync(queue, 0, 2 * b.steps.size() * sizeof(int), s), "cudaMemsetAsync");
   launch_batch_prepare(P, I + b.all.item_off, b.all.n_items, b.all.n_units, true, s);
   check_launch(s);
   ++n;
   for (size_t t = 0; t < b.steps.size(); ++t)
   {
     const fir_batch::Step& st = b.steps[t];
-    batch_project(b, st.proj, queue + t, b.shape, s);
+    batch_project(b, st.proj, queue + 2 * t, b.shape, false, s);
+    n += st.proj.n_items > 0 ? 1 : 0;
+    if (st.proj_f.n_items > 0)
+    {
+      batch_project(b, st.proj_f, queue + 2 * t + 1, b.shape, true, s);
+      ++n;
+    }
     launch_batch_em(P, I + st.em.item_off, st.em.n_items, st.em.n_units, s);
     check_launch(s);
-    n += 2;
+    ++n;
     if (st.filt.n_items > 0)
     {
       for (int axis = 0; axis < 3; ++axis)
@@ -268,9 +277,13 @@ fir_status fir_batch_create(fir_batch** out, fir_ctx* ctx, int n_problems, const
       q.off_sino = take((size_t)q.p.g.n_bins * sizeof(float));
       q.off_sens = take(nv * q.n_subsets * sizeof(float));
       q.off_img = take(nv * sizeof(float));
-      q.off_wide = take(nv * sizeof(double));
+      {
+        const Grid g = grid_of(c, q.v);
+        q.exchanged = use_exchanged(c, g);
+        q.gather_float = !q.exchanged && !use_exchanged(c, g, 12.0) && use_exchanged(c, g, 8.0);
+      }
+      q.off_wide = take(q.gather_float ? 0 : nv * sizeof(double));
       q.off_bp = take(nv * sizeof(float));
-      q.exchanged = use_exchanged(c, grid_of(c, q.v));
       q.off_wide_t = take(q.exchanged ? nv * sizeof(double) : 0);
       q.off_bp_t = take(q.exchanged ? nv * sizeof(float) : 0);
       q.off_t1 = take(q.filter ? nv * sizeof(float) : 0);
@@ -304,7 +317,7 @@ fir_status fir_batch_create(fir_batch** out, fir_ctx* ctx, int n_problems, const
         d.bias = nullptr;
         d.sens = reinterpret_cast<const float*>(base + q.off_sens);
         d.img = reinterpret_cast<float*>(base + q.off_img);
-        d.wide = reinterpret_cast<double*>(base + q.off_wide);
+        d.wide = q.gather_float ? nullptr : reinterpret_cast<double*>(base + q.off_wide);
         d.bp = reinterpret_cast<float*>(base + q.off_bp);
         d.wide_t = q.exchanged ? reinterpret_cast<double*>(base + q.off_wide_t) : nullptr;
         d.bp_t = q.exchanged ? reinterpret_cast<float*>(base + q.off_bp_t) : nullptr;
@@ -343,7 +356,7 @@ fir_status fir_batch_create(fir_batch** out, fir_ctx* ctx, int n_problems, const
       }
       for (int t = 0; t < n_steps; ++t)
       {
-        std::vector<int> probs, subs, filts, fprobs, fsubs, fflags;
+        std::vector<int> probs, subs, filts, fprobs, fsubs, fflags, dprobs, dsubs, dfilts, gprobs, gsubs, gfilts;
         for (int k : order)
         {
           const fir_batch::Problem& q = b->pr[(size_t)k];
@@ -356,6 +369,9 @@ fir_status fir_batch_create(fir_batch** out, fir_ctx* ctx, int n_problems, const
           probs.push_back(k);
           subs.push_back(t % q.n_subsets);
           filts.push_back(f);
+          (q.gather_float ? gprobs : dprobs).push_back(k);
+          (q.gather_float ? gsubs : dsubs).push_back(t % q.n_subsets);
+          (q.gather_float ? gfilts : dfilts).push_back(f);
           if (f)
           {
             fprobs.push_back(k);
@@ -364,7 +380,8 @@ fir_status fir_batch_create(fir_batch** out, fir_ctx* ctx, int n_problems, const
           }
         }
         fir_batch::Step st;
-        st.proj = add_launch(items, probs, subs, filts, lor_units);
+        st.proj = add_launch(items, dprobs, dsubs, dfilts, lor_units);
+        st.proj_f = add_launch(items, gprobs, gsubs, gfilts, lor_units);
         st.em = add_launch(items, probs, subs, filts, vox_units);
         st.filt = add_launch(items, fprobs, fsubs, fflags, vox_units);
         b->steps.push_back(st);
@@ -373,12 +390,13 @@ fir_status fir_batch_create(fir_batch** out, fir_ctx* ctx, int n_problems, const
       batch_copy(*b, b->desc.p, b->desc_host.data(), b->desc_host.size() * sizeof(BatchProblem));
       b->items.ensure(std::max<size_t>(items.size(), 1) * sizeof(BatchItem));
       batch_copy(*b, b->items.p, items.data(), items.size() * sizeof(BatchItem));
-      b->queue.ensure(std::max<size_t>(b->steps.size(), 1) * sizeof(int));
+      b->queue.ensure(std::max<size_t>(2 * b->steps.size(), 1) * sizeof(int));
       cuda_ok(cudaStreamSynchronize(c.stream), "cudaStreamSynchronize");
       b->schedule_launches = 1;
       for (const auto& st : b->steps)
       {
-        b->schedule_launches += 2 + (st.filt.n_items > 0 ? 3 : 0);
+        b->schedule_launches += 1 + (st.proj.n_items > 0 ? 1 : 0) + (st.proj_f.n_items > 0 ? 1 : 0) +
+                                (st.filt.n_items > 0 ? 3 : 0);
       }
     }
     catch (...)
@@ -564,7 +582,10 @@ fir_status fir_batch_tune(fir_batch* batch, double* best_ms)
           check_launch(b.stream);
           cuda_ok(cudaMemsetAsync(queue, 0, sizeof(int), b.stream), "cudaMemsetAsync");
           cuda_ok(cudaEventRecord(e0, b.stream), "cudaEventRecord");
-          batch_project(b, b.steps[0].proj, queue, L, b.stream);
+          // step 0's projector: the double-gather launch, or the float one
+          // when every problem gathers floats
+          const bool f = b.steps[0].proj.n_items == 0;
+          batch_project(b, f ? b.steps[0].proj_f : b.steps[0].proj, queue, L, f, b.stream);
           cuda_ok(cudaEventRecord(e1, b.stream), "cudaEventRecord");
           cuda_ok(cudaEventSynchronize(e1), "cudaEventSynchronize");
           float ms = 0.0f;

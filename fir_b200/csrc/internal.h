@@ -43,6 +43,10 @@ void launch_backward(const Grid& g, const Sino& s, const Tables& t, const float*
 void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const double* img, const double* img_t,
                         const float* sino, const float* mult, const float* bias, float* bp, float* bp_t,
                         bool skip_zero, const LaunchCfg& cfg);
+// The same (one orientation), gathering from the float image itself.
+void launch_osem_subset_float_image(const Grid& g, const Sino& s, const Tables& t, const float* img,
+                                    const float* sino, const float* mult, const float* bias, float* bp,
+                                    bool skip_zero, const LaunchCfg& cfg);
 void launch_siddon_paths(const Grid& g, long long n, const double* ends, int cap, int* coords,
                          double* lengths, int* counts, int* crosses, const LaunchCfg& cfg);
 void launch_lor_paths(const Grid& g, const Sino& s, const Tables& t, long long n,
@@ -124,7 +128,7 @@ struct BatchProblem
   const float* bias;  // nullptr: none
   const float* sens;  // n_subsets frames
   float* img;
-  double* wide;  // double copy of img for the projector gathers
+  double* wide;  // double copy of img for the projector gathers (null: it gathers img itself)
   float* bp;
   double* wide_t;  // wide and bp with x and y exchanged ([z][x][y]), for LORs
   float* bp_t;     // running mostly along x; bp_t is added into bp by the EM step
@@ -162,9 +166,11 @@ struct BatchLaunch
 void launch_batch_prepare(const BatchProblem* P, const BatchItem* items, int n_items, int n_units,
                           bool write_img, cudaStream_t stream);
 // bp += backprojection of measured/estimated for every item's subset.
-// queue: a zeroed counter (persistent mode).
+// queue: a zeroed counter (persistent mode).  gather_float: the items'
+// problems have no double copy (wide == null) and gather their float images.
 void launch_batch_project(const BatchProblem* P, const BatchItem* items, int n_items, int n_bundles,
-                          int* queue, const BatchLaunch& L, int n_sms, int* check, cudaStream_t stream);
+                          int* queue, const BatchLaunch& L, int n_sms, int* check, bool gather_float,
+                          cudaStream_t stream);
 // Gated EM update of img; bp <- 0.  Items without filtering also apply the
 // cut and refresh wide.
 void launch_batch_em(const BatchProblem* P, const BatchItem* items, int n_items, int n_units,

@@ -32,9 +32,13 @@ __device__ __forceinline__ void flag(int* check, int bit)
 // into bp_t: the 32 parallel LORs of a warp are then offset along the
 // contiguous axis, so each warp-wide gather and atomic touches about half as
 // many cache lines.  The caller adds bp_t back into bp.
-template<bool kWeighted>
+//
+// TImg: the image the projection gathers from, the double copy or the float
+// image itself (widened per step, exact; for volumes whose double copy does
+// not fit in L2 beside the accumulator).
+template<bool kWeighted, typename TImg = double>
 __device__ __forceinline__ void osem_lor_body(const Grid& g, const Sino& s, int subset, const Tables& t,
-                                              const double* __restrict__ img, const double* __restrict__ img_t,
+                                              const TImg* __restrict__ img, const TImg* __restrict__ img_t,
                                               const float* __restrict__ sino, const float* __restrict__ mult,
                                               const float* __restrict__ bias, float* bp, float* bp_t,
                                               bool skip_zero, int i, int* check)
@@ -59,7 +63,7 @@ __device__ __forceinline__ void osem_lor_body(const Grid& g, const Sino& s, int 
       go = siddon_setup(g, e, w, tr);
     }
   }
-  const double* im = tr ? img_t : img;
+  const TImg* im = tr ? img_t : img;
   float* b = tr ? bp_t : bp;
   // b may come from a descriptor in memory, not a kernel parameter: without
   // this the compiler cannot tell the atomic's address space and tests it at
@@ -69,7 +73,7 @@ __device__ __forceinline__ void osem_lor_body(const Grid& g, const Sino& s, int 
   bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
     if (inside)
     {
-      line = accumulate(line, len, __ldg(im + c));
+      line = accumulate(line, len, (double)__ldg(im + c));
     }
   });
   __syncwarp();

@@ -114,17 +114,18 @@ __global__ void __launch_bounds__(256) k_backward(Grid g, Sino s, Tables t,
 
 // One OSEM sub-iteration over the subset of s: one thread per enumerated
 // LOR (reconAlgos.cc:119-158); kWeighted adds the multiplicative factors.
-template<bool kWeighted>
+template<bool kWeighted, typename TImg>
 __global__ void __launch_bounds__(256, 4) k_osem_subset(Grid g, Sino s, Tables t,
-                                                        const double* __restrict__ img,
-                                                        const double* __restrict__ img_t,
+                                                        const TImg* __restrict__ img,
+                                                        const TImg* __restrict__ img_t,
                                                         const float* __restrict__ sino,
                                                         const float* __restrict__ mult,
                                                         const float* __restrict__ bias, float* bp, float* bp_t,
                                                         int skip_zero, int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  osem_lor_body<kWeighted>(g, s, s.subset, t, img, img_t, sino, mult, bias, bp, bp_t, skip_zero != 0, i, check);
+  osem_lor_body<kWeighted, TImg>(g, s, s.subset, t, img, img_t, sino, mult, bias, bp, bp_t, skip_zero != 0, i,
+                                 check);
 }
 
 // Path dump of one segment into row i of coords / lengths.
@@ -251,13 +252,34 @@ void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const dou
   const unsigned nb = blocks_for(s.n_enum, cfg.block);
   if (mult != nullptr)
   {
-    k_osem_subset<true><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, img_t, sino, mult, bias, bp, bp_t,
-                                                          skip_zero ? 1 : 0, cfg.check);
+    k_osem_subset<true, double><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, img_t, sino, mult, bias, bp, bp_t,
+                                                                  skip_zero ? 1 : 0, cfg.check);
   }
   else
   {
-    k_osem_subset<false><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, img_t, sino, nullptr, bias, bp, bp_t,
-                                                           skip_zero ? 1 : 0, cfg.check);
+    k_osem_subset<false, double><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, img_t, sino, nullptr, bias, bp,
+                                                                   bp_t, skip_zero ? 1 : 0, cfg.check);
+  }
+}
+
+void launch_osem_subset_float_image(const Grid& g, const Sino& s, const Tables& t, const float* img,
+                                    const float* sino, const float* mult, const float* bias, float* bp,
+                                    bool skip_zero, const LaunchCfg& cfg)
+{
+  if (s.n_enum == 0)
+  {
+    return;
+  }
+  const unsigned nb = blocks_for(s.n_enum, cfg.block);
+  if (mult != nullptr)
+  {
+    k_osem_subset<true, float><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, nullptr, sino, mult, bias, bp,
+                                                                 nullptr, skip_zero ? 1 : 0, cfg.check);
+  }
+  else
+  {
+    k_osem_subset<false, float><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, nullptr, sino, nullptr, bias, bp,
+                                                                  nullptr, skip_zero ? 1 : 0, cfg.check);
   }
 }
 
