@@ -219,6 +219,52 @@ __global__ void __launch_bounds__(256) k_ratio(Grid g, Sino s, Tables t, const d
   }
 }
 
+// Greedy chunks of whole LORs: chunk k is [b_k, b_k+1), with b_k+1 the
+// largest index whose offset stays within max_pairs of b_k's (at least
+// b_k + 1).  max_pairs = min(total, cap), at least floor_pairs.  out: total,
+// max_pairs, the number of chunks K, unused, then the (index, offset) of
+// b_0 .. b_K.  One thread: a binary search per chunk, so that the host reads
+// a few numbers instead of every LOR's offset.
+__global__ void k_chunks(const long long* __restrict__ offsets, const int* __restrict__ counts, long long n,
+                         long long cap, long long floor_pairs, long long* out)
+{
+  if (blockIdx.x != 0 || threadIdx.x != 0)
+  {
+    return;
+  }
+  const long long total = offsets[n - 1] + counts[n - 1];
+  long long mp = total < cap ? total : cap;
+  mp = mp < floor_pairs ? floor_pairs : mp;
+  auto off = [&](long long i) { return i < n ? offsets[i] : total; };
+  long long first = 0, k = 0;
+  out[4] = 0;
+  out[5] = 0;
+  while (first < n)
+  {
+    const long long limit = off(first) + mp;
+    long long lo = first + 1, hi = n;
+    if (off(lo) <= limit)
+    {
+      while (lo < hi)
+      {
+        const long long mid = (lo + hi + 1) >> 1;
+        if (off(mid) <= limit)
+          lo = mid;
+        else
+          hi = mid - 1;
+      }
+    }
+    first = lo;
+    ++k;
+    out[4 + 2 * k] = first;
+    out[5 + 2 * k] = off(first);
+  }
+  out[0] = total;
+  out[1] = mp;
+  out[2] = k;
+  out[3] = 0;
+}
+
 int bits_for(long long n)
 {
   int b = 1;
@@ -268,8 +314,10 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
   {
     return e;
   }
+  // chunk table: 4 header words and (index, offset) of up to n + 1 bounds
+  const size_t chunk_words = 4 + 2 * ((size_t)n + 1);
   unsigned char* idx = static_cast<unsigned char*>(scratch(0, round256((size_t)n * 4) + round256((size_t)n * 8) +
-                                                                 round256(scan_bytes)));
+                                                                 round256(scan_bytes) + round256(chunk_words * 8)));
   if (idx == nullptr)
   {
     return cudaErrorMemoryAllocation;
@@ -277,18 +325,22 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
   int* counts = reinterpret_cast<int*>(idx);
   long long* offsets = reinterpret_cast<long long*>(idx + round256((size_t)n * 4));
   void* scan_tmp = idx + round256((size_t)n * 4) + round256((size_t)n * 8);
+  long long* chunk_dev =
+    reinterpret_cast<long long*>(idx + round256((size_t)n * 4) + round256((size_t)n * 8) + round256(scan_bytes));
   k_count<<<blocks_for(n, cfg.block), cfg.block, 0, cfg.stream>>>(g, s, t, vals, vals_by_enum ? 1 : 0, counts,
                                                                   cfg.check);
   e = cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, counts, offsets, (int)n, cfg.stream);
-  std::vector<long long> off((size_t)n + 1);
-  int last_count = 0;
   if (e == cudaSuccess)
   {
-    e = cudaMemcpyAsync(off.data(), offsets, (size_t)n * 8, cudaMemcpyDeviceToHost, cfg.stream);
+    k_chunks<<<1, 32, 0, cfg.stream>>>(offsets, counts, n, max_pairs_cap, (long long)g.guard + 8, chunk_dev);
+    e = cudaGetLastError();
   }
+  // the header and the first bounds in one read; the rest, if there are more
+  constexpr size_t kFirstWords = 4 + 2 * 64;
+  std::vector<long long> chunk(std::min(chunk_words, kFirstWords));
   if (e == cudaSuccess)
   {
-    e = cudaMemcpyAsync(&last_count, counts + n - 1, 4, cudaMemcpyDeviceToHost, cfg.stream);
+    e = cudaMemcpyAsync(chunk.data(), chunk_dev, chunk.size() * 8, cudaMemcpyDeviceToHost, cfg.stream);
   }
   if (e == cudaSuccess)
   {
@@ -298,21 +350,31 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
   {
     return e;
   }
-  off[(size_t)n] = off[(size_t)n - 1] + last_count;
-  *launches += 2;
-  const long long total = off[(size_t)n];
+  *launches += 3;
+  const long long total = chunk[0];
   if (total == 0)
   {
     return cudaGetLastError();
   }
+  const size_t used_words = 4 + 2 * ((size_t)chunk[2] + 1);
+  if (used_words > chunk.size())
+  {
+    chunk.resize(used_words);
+    e = cudaMemcpyAsync(chunk.data() + kFirstWords, chunk_dev + kFirstWords, (used_words - kFirstWords) * 8,
+                        cudaMemcpyDeviceToHost, cfg.stream);
+    if (e == cudaSuccess)
+    {
+      e = cudaStreamSynchronize(cfg.stream);
+    }
+    if (e != cudaSuccess)
+    {
+      return e;
+    }
+  }
 
   // 2. pair buffers for chunks of at most max_pairs (at least one LOR's
   // padded path)
-  long long max_pairs = total < max_pairs_cap ? total : max_pairs_cap;
-  if (max_pairs < g.guard + 8)
-  {
-    max_pairs = g.guard + 8;
-  }
+  const long long max_pairs = chunk[1];
   // runs of one chunk: at most one per voxel, the padding run, and one per pair
   const long long max_runs = max_pairs < n_vox + 1 ? max_pairs : n_vox + 1;
   size_t sort_bytes = 0, rle_bytes = 0, run_scan_bytes = 0;
@@ -354,20 +416,15 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
 
   // 3. chunks of whole LORs, reduced in order
   const int key_bits = bits_for(n_vox + 1);  // the padding key n_vox included
-  long long first = 0;
-  while (first < n)
+  for (long long c = 0; c < chunk[2]; ++c)
   {
-    long long last = first + 1;
-    while (last < n && off[(size_t)last + 1] - off[(size_t)first] <= max_pairs)
-    {
-      ++last;
-    }
-    const long long m = off[(size_t)last] - off[(size_t)first];
+    const long long first = chunk[(size_t)(4 + 2 * c)], last = chunk[(size_t)(6 + 2 * c)];
+    const long long base = chunk[(size_t)(5 + 2 * c)];
+    const long long m = chunk[(size_t)(7 + 2 * c)] - base;
     if (m > 0)
     {
       k_emit<<<blocks_for(last - first, kEmitBlock), kEmitBlock, 0, cfg.stream>>>(
-        g, s, t, vals, vals_by_enum ? 1 : 0, (int)first, (int)last, offsets, off[(size_t)first], (unsigned)n_vox,
-        keys_a, prods_a);
+        g, s, t, vals, vals_by_enum ? 1 : 0, (int)first, (int)last, offsets, base, (unsigned)n_vox, keys_a, prods_a);
       size_t tmp = tmp_bytes;
       e = cub::DeviceRadixSort::SortPairs(sort_tmp, tmp, keys_a, keys_b, prods_a, prods_b, (int)m, 0, key_bits,
                                           cfg.stream);
@@ -392,7 +449,6 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
                                                                       prods_b, (unsigned)n_vox, img);
       *launches += 2;
     }
-    first = last;
   }
   return cudaGetLastError();
 }
