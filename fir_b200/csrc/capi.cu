@@ -451,7 +451,7 @@ void drain_timing(fir_ctx& c)
 // Deterministic-mode backprojection of vals (per bin, or per enumerated LOR
 // when by_enum) into img, FIR's serial order; scratch from the context.
 void det_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, const float* vals, bool by_enum,
-                     float* img, long long nvox)
+                     float* img, long long nvox, const int* counts = nullptr)
 {
   const ScratchFn scratch = [&c](int slot, size_t bytes) -> void* {
     DevBuf& b = slot == 0 ? c.det : c.det_pairs;
@@ -467,7 +467,8 @@ void det_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, 
   long long launches = 0;
   // chunks of at most det_chunk pairs (default 2^28: about 6 GiB of keys,
   // products and sort buffers)
-  cuda_ok(deterministic_backproject(g, s, t, vals, by_enum, img, scratch, c.det_chunk, nvox, cfg_of(c), &launches),
+  cuda_ok(deterministic_backproject(g, s, t, vals, by_enum, counts, img, scratch, c.det_chunk, nvox, cfg_of(c),
+                                    &launches),
           "deterministic backprojection");
   c.launches += launches;
 }
@@ -536,9 +537,12 @@ void ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t
   if (c.backproj == FIR_BACKPROJ_DETERMINISTIC)
   {
     const double* wimg = widen(c, img, nvox);
-    float* ratio = static_cast<float*>(c.ratio.ensure((size_t)std::max(s.n_enum, 1) * sizeof(float)));
-    timed_launch(c, [&] { launch_ratio(g, s, t, wimg, sino, mult, bias, ratio, cfg_of(c)); });
-    det_backproject(c, g, s, t, ratio, true, bp, nvox);
+    // the ratio and, from the same walks, the pair count of every LOR
+    const size_t ne = (size_t)std::max(s.n_enum, 1);
+    float* ratio = static_cast<float*>(c.ratio.ensure(ne * (sizeof(float) + sizeof(int))));
+    int* counts = reinterpret_cast<int*>(ratio + ne);
+    timed_launch(c, [&] { launch_ratio(g, s, t, wimg, sino, mult, bias, ratio, counts, cfg_of(c)); });
+    det_backproject(c, g, s, t, ratio, true, bp, nvox, counts);
     return;
   }
   if (!use_exchanged(c, g))

@@ -172,9 +172,14 @@ __global__ void __launch_bounds__(256) k_reduce_runs(const int* __restrict__ n_r
 // (reconAlgos.cc:119-158): measured / (projection + bias) when that exceeds
 // 1e-5, else 0; with multiplicative factors m, m * measured / (m * projection
 // + bias).
+//
+// With counts, the kernel also writes what k_count would for the ratio: the
+// LOR's element count rounded up to a multiple of 8, 0 where the ratio is 0
+// (its walk is the one the backprojection will take).
 __global__ void __launch_bounds__(256) k_ratio(Grid g, Sino s, Tables t, const double* __restrict__ img,
                                                const float* __restrict__ sino, const float* __restrict__ mult,
-                                               const float* __restrict__ bias, float* ratio, int* check)
+                                               const float* __restrict__ bias, float* ratio, int* counts,
+                                               int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < s.n_enum;
@@ -189,10 +194,12 @@ __global__ void __launch_bounds__(256) k_ratio(Grid g, Sino s, Tables t, const d
     go = siddon_setup(g, e, w);
   }
   float line = 0.0f;
+  int k = 0;
   const bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
     if (inside)
     {
       line = accumulate(line, len, __ldg(img + c));
+      ++k;
     }
   });
   if (!ok && check != nullptr)
@@ -216,6 +223,10 @@ __global__ void __launch_bounds__(256) k_ratio(Grid g, Sino s, Tables t, const d
       q = __fmul_rn(q, m);
     }
     ratio[i] = q;
+    if (counts != nullptr)
+    {
+      counts[i] = q != 0.0f ? (k + 7) & ~7 : 0;
+    }
   }
 }
 
@@ -282,12 +293,12 @@ unsigned blocks_for(long long n, int block)
 }  // namespace
 
 void launch_ratio(const Grid& g, const Sino& s, const Tables& t, const double* img, const float* sino,
-                  const float* mult, const float* bias, float* ratio, const LaunchCfg& cfg)
+                  const float* mult, const float* bias, float* ratio, int* counts, const LaunchCfg& cfg)
 {
   if (s.n_enum > 0)
   {
     k_ratio<<<blocks_for(s.n_enum, cfg.block), cfg.block, 0, cfg.stream>>>(g, s, t, img, sino, mult, bias, ratio,
-                                                                          cfg.check);
+                                                                          counts, cfg.check);
   }
 }
 
@@ -297,7 +308,7 @@ size_t round256(size_t b) { return (b + 255) / 256 * 256; }
 }  // namespace
 
 cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables& t, const float* vals,
-                                      bool vals_by_enum, float* img, const ScratchFn& scratch,
+                                      bool vals_by_enum, const int* counts_in, float* img, const ScratchFn& scratch,
                                       long long max_pairs_cap, long long n_vox, const LaunchCfg& cfg,
                                       long long* launches)
 {
@@ -323,16 +334,21 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
     return cudaErrorMemoryAllocation;
   }
   int* counts = reinterpret_cast<int*>(idx);
+  const int* cnt = counts_in != nullptr ? counts_in : counts;
   long long* offsets = reinterpret_cast<long long*>(idx + round256((size_t)n * 4));
   void* scan_tmp = idx + round256((size_t)n * 4) + round256((size_t)n * 8);
   long long* chunk_dev =
     reinterpret_cast<long long*>(idx + round256((size_t)n * 4) + round256((size_t)n * 8) + round256(scan_bytes));
-  k_count<<<blocks_for(n, cfg.block), cfg.block, 0, cfg.stream>>>(g, s, t, vals, vals_by_enum ? 1 : 0, counts,
-                                                                  cfg.check);
-  e = cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, counts, offsets, (int)n, cfg.stream);
+  if (counts_in == nullptr)
+  {
+    k_count<<<blocks_for(n, cfg.block), cfg.block, 0, cfg.stream>>>(g, s, t, vals, vals_by_enum ? 1 : 0, counts,
+                                                                    cfg.check);
+    *launches += 1;
+  }
+  e = cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, cnt, offsets, (int)n, cfg.stream);
   if (e == cudaSuccess)
   {
-    k_chunks<<<1, 32, 0, cfg.stream>>>(offsets, counts, n, max_pairs_cap, (long long)g.guard + 8, chunk_dev);
+    k_chunks<<<1, 32, 0, cfg.stream>>>(offsets, cnt, n, max_pairs_cap, (long long)g.guard + 8, chunk_dev);
     e = cudaGetLastError();
   }
   // the header and the first bounds in one read; the rest, if there are more
@@ -350,7 +366,7 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
   {
     return e;
   }
-  *launches += 3;
+  *launches += 2;
   const long long total = chunk[0];
   if (total == 0)
   {

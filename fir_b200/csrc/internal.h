@@ -55,18 +55,20 @@ void launch_lor_paths(const Grid& g, const Sino& s, const Tables& t, long long n
 
 // deterministic.cu
 // ratio[i] = sino / (projection + bias) for enumerated LOR i, or 0
-// (with mult: m * sino / (m * projection + bias))
+// (with mult: m * sino / (m * projection + bias)); counts (or null): the
+// pair counts deterministic_backproject needs for that ratio.
 void launch_ratio(const Grid& g, const Sino& s, const Tables& t, const double* img, const float* sino,
-                  const float* mult, const float* bias, float* ratio, const LaunchCfg& cfg);
+                  const float* mult, const float* bias, float* ratio, int* counts, const LaunchCfg& cfg);
 // Device scratch of at least `bytes` for slot 0 (per-LOR counts and
 // offsets) or slot 1 (pairs and sort space); nullptr if unavailable.
 using ScratchFn = std::function<void*(int slot, size_t bytes)>;
 // img += backprojection of vals (per bin, or per enumerated LOR; nullptr =
 // all ones), summed in FIR's serial LOR order with FIR's rounding, in
-// chunks of at most max_pairs_cap (voxel, product) pairs.  Synchronises the
-// stream once, after counting.
+// chunks of at most max_pairs_cap (voxel, product) pairs.  counts_in (or
+// null): per-LOR pair counts from launch_ratio for these vals.  Synchronises
+// the stream once, after counting.
 cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables& t, const float* vals,
-                                      bool vals_by_enum, float* img, const ScratchFn& scratch,
+                                      bool vals_by_enum, const int* counts_in, float* img, const ScratchFn& scratch,
                                       long long max_pairs_cap, long long n_vox, const LaunchCfg& cfg,
                                       long long* launches);
 
