@@ -276,6 +276,12 @@ __global__ void k_chunks(const long long* __restrict__ offsets, const int* __res
   out[3] = 0;
 }
 
+// 64-bit sum of pair counts, for the offsets scan.
+struct PairSum
+{
+  __host__ __device__ long long operator()(long long a, long long b) const { return a + b; }
+};
+
 int bits_for(long long n)
 {
   int b = 1;
@@ -319,8 +325,10 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
   }
   // 1. path element count of every LOR and their exclusive prefix sum
   size_t scan_bytes = 0;
-  cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (const int*)nullptr, (long long*)nullptr,
-                                                (int)n, cfg.stream);
+  // offsets exceed 2^31 pairs on large subsets: the scan must accumulate in
+  // 64 bits (ExclusiveSum would accumulate in the counts' int type)
+  cudaError_t e = cub::DeviceScan::ExclusiveScan(nullptr, scan_bytes, (const int*)nullptr, (long long*)nullptr,
+                                                 PairSum{}, 0LL, (int)n, cfg.stream);
   if (e != cudaSuccess)
   {
     return e;
@@ -345,7 +353,7 @@ cudaError_t deterministic_backproject(const Grid& g, const Sino& s, const Tables
                                                                     cfg.check);
     *launches += 1;
   }
-  e = cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, cnt, offsets, (int)n, cfg.stream);
+  e = cub::DeviceScan::ExclusiveScan(scan_tmp, scan_bytes, cnt, offsets, PairSum{}, 0LL, (int)n, cfg.stream);
   if (e == cudaSuccess)
   {
     k_chunks<<<1, 32, 0, cfg.stream>>>(offsets, cnt, n, max_pairs_cap, (long long)g.guard + 8, chunk_dev);

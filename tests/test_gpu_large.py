@@ -10,7 +10,11 @@ real extents:
 * on all LORs, the adjoint test holds, and so does exact linearity under
   scaling by two;
 * one OSEM iteration (32 subsets) run as one captured graph (a batch of one
-  problem) matches fir_osem within 1e-5 relative L2.
+  problem) matches fir_osem within 1e-5 relative L2;
+* the volume's double copy does not fit in L2 beside the accumulator, so the
+  fused kernel gathers the float image: one subset's backprojected ratio
+  matches the deterministic mode, which gathers the double copy and sums in
+  FIR's order, within the 1e-6 relative L2 of float atomic order.
 """
 import numpy as np
 import pytest
@@ -89,3 +93,22 @@ def test_one_iteration_graph_matches_plain(large):
     assert np.isfinite(got).all() and float(want.max()) > 0
     assert np.linalg.norm(got - want) <= 1e-5 * np.linalg.norm(want)
     batch.close()
+
+
+def test_float_gather_subset_matches_deterministic(large):
+    w, ctx = large
+    g = torch.Generator(device=DEV).manual_seed(5)
+    img = torch.rand(w.vol.shape_zyx, generator=g, device=DEV) + 0.5
+    y = torch.poisson(torch.full((w.n_lors,), 3.0, device=DEV), generator=g)
+    got = torch.zeros_like(img)
+    ctx.ratio_backprojection(w.proj, y, w.vol, img, got, w.osem.n_subsets, 3)
+    det = capi.Context(w.scanner)
+    det.set_option(capi.FIR_OPT_GEOMETRY, capi.FIR_GEOMETRY_EXACT)
+    det.set_option(capi.FIR_OPT_BACKPROJ_MODE, capi.FIR_BACKPROJ_DETERMINISTIC)
+    want = torch.zeros_like(img)
+    det.ratio_backprojection(w.proj, y, w.vol, img, want, w.osem.n_subsets, 3)
+    torch.cuda.synchronize()
+    det.close()
+    assert float(want.max()) > 0
+    rel = float((got.double() - want.double()).norm() / want.double().norm())
+    assert rel <= 1e-6
