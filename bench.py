@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--workload", choices=["clinical", "small", "large"], default="clinical")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-runs", type=int, default=3, help="timed fir_osem calls of the e2e leg (median)")
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--det-steps", type=int, default=2,
                     help="extra sub-iterations timed with deterministic backprojection (0: skip)")
@@ -156,18 +157,17 @@ def subset_of_bins(proj, n_subsets, torch, device):
     return torch.cat(parts)
 
 
-def reference_counts(w, cache_dir="/tmp"):
+def reference_counts(w, ref, n_bins, cache_dir="/tmp"):
     """Path elements per bin by FIR's own Siddon (oracle/_ref, all threads)."""
     import numpy as np
-
-    from oracle.bridge import Reference
 
     key = f"{w.name}_{w.proj.n_rings}_{w.proj.n_crystals_per_ring}_{w.proj.n_tang_coords}_{w.vol.size[0]}"
     path = os.path.join(cache_dir, f"fir_counts_{key}.npy")
     if os.path.exists(path):
-        return np.load(path)
-    ref = Reference()
-    c = ref.path_counts(w.scanner, w.proj, w.vol, w.n_lors)
+        c = np.load(path)
+        if c.size == n_bins:
+            return c
+    c = ref.path_counts(w.scanner, w.proj, w.vol, n_bins)
     try:
         np.save(path, c)
     except Exception:
@@ -175,32 +175,58 @@ def reference_counts(w, cache_dir="/tmp"):
     return c
 
 
+def bench_config(w, world, n_bins):
+    """The `config` object of the JSON line, the same for both arms."""
+    nsub = w.osem.n_subsets
+    return {
+        "workload": f"{w.name}: OSEM sub-iteration, {w.proj.n_rings} rings x {w.proj.n_crystals_per_ring} "
+                    f"crystals, {w.proj.n_tang_coords} tangential bins, {n_bins} LORs, "
+                    f"{'x'.join(str(s) for s in w.vol.size)} @ {w.vol.voxel[0]} mm, {nsub} subsets, "
+                    f"FWHM {w.osem.fwhm_xyz[0]} mm, seeded phantom, water attenuation, "
+                    f"{w.counts:.0e} Poisson counts",
+        "l2": "flushed (256 MB write) before every timed step, outside the step's events",
+        "parallelism": f"views of each subset split over {world} GPUs, NCCL all-reduce of the backprojection"
+                       if world > 1 else "single GPU",
+    }
+
+
 # ------------------------------------------------------------ CPU reference
 
-def cpu_reference_run(w, steps_budget: int, verbose=False):
-    """Times FIR's reconAlgos::OSEM on host cores: `iters` full iterations
-    (16 sub-iterations each) of the clinical workload from a uniform image.
-    Measured data are seeded Poisson(15) counts and the sensitivity is
-    uniform: step counts and timing do not depend on data values, and with
-    every LOR crossing the positive image every crossing LOR is backprojected
-    (S_bwd = S_fwd)."""
+def reference_inputs(w, ref):
+    """The benchmark's measured data and sensitivity made by FIR's own
+    compiled code (oracle/_ref): HU-to-mu map, forward projections of the
+    mu map and of the phantom, and the subsets' sensitivity.  The sinogram
+    is bit-identical to the GPU arm's (both forward projectors are
+    bit-identical to FIR and the rest is workloads.measured_sinogram)."""
+    from fir_b200 import workloads
+
+    nb = ref.proj_geometry(w.proj)["n_bins"]
+    mu = ref.hu_to_mu(w.vol, workloads.hounsfield(w))
+    line_mu = ref.forward(w.scanner, w.proj, w.vol, mu, nb)
+    ax = ref.forward(w.scanner, w.proj, w.vol, workloads.activity(w), nb)
+    y = workloads.measured_sinogram(w, ax, line_mu)
+    sens = ref.sensitivity(w.scanner, w.proj, w.vol, w.osem.n_subsets)
+    return nb, y, sens
+
+
+def cpu_reference_run(w, ref, y, sens, img0, counts, iters):
+    """Times FIR's reconAlgos::OSEM (oracle/_ref, all host threads) for
+    `iters` full iterations of the workload on the given data, sensitivity
+    and start image.  Steps are counted as FIR enumerates them: every path
+    element of every LOR for the projection, and for the backprojection
+    every element of every crossing LOR (exact from a uniform start image,
+    where every crossing LOR's estimate is positive; an upper bound after
+    that, which favours FIR)."""
     import numpy as np
 
     from fir_b200.geometry import OSEMParams
-    from oracle.bridge import Reference
 
-    ref = Reference()
     cores = os.cpu_count() or 1
     ref.threads(cores)
-    counts = reference_counts(w)
-    nb = counts.size
-    y = np.random.default_rng(w.seed).poisson(15.0, nb).astype(np.float32)
     nsub = w.osem.n_subsets
-    sens = np.ones((nsub,) + tuple(w.vol.shape_zyx), np.float32)
-    img = np.ones(w.vol.shape_zyx, np.float32)
+    img = np.ascontiguousarray(img0, np.float32)
     prm = OSEMParams(n_iterations=1, n_subsets=nsub, convolution_interval=w.osem.convolution_interval,
                      fwhm_xyz=list(w.osem.fwhm_xyz), cut_radius=w.osem.cut_radius)
-    iters = max(1, int(math.ceil(steps_budget / nsub)))
     t0 = time.perf_counter()
     for _ in range(iters):
         img = ref.osem(w.scanner, w.proj, w.vol, y, img, sens, prm)
@@ -213,12 +239,16 @@ def cpu_reference_run(w, steps_budget: int, verbose=False):
         "kind": "reference",
         "seconds": dt,
         "osem_s_per_iteration": dt / iters,
-        "sample": f"{iters} full OSEM iteration(s) of the clinical workload ({nsub} sub-iterations each) by "
-                  f"FIR's reconAlgos::OSEM compiled -O3 -fopenmp, {cores} threads; S = {steps} ray-voxel steps",
+        "sample": f"{iters} full OSEM iteration(s) of the {w.name} workload ({nsub} sub-iterations each) by "
+                  f"FIR's reconAlgos::OSEM compiled -O3 -fopenmp, {cores} threads, on the same measured data "
+                  f"and sensitivity as the GPU arm; S = {steps} ray-voxel steps",
     }
 
 
 def reference_arm(args, rank):
+    """FIR's own OpenMP implementation of the path (oracle/_ref), on the host
+    cores, on the GPU arm's workload, data and config.  Nothing of fir_b200's
+    native library is loaded in this process."""
     if rank != 0:
         return 0
     w = workload(args.workload)
@@ -226,15 +256,23 @@ def reference_arm(args, rank):
         from oracle import bridge
 
         if not bridge.reference_available():
-            bridge.build(reference=True)
-        if not bridge.reference_available():
             raise FileNotFoundError("oracle/_ref/libfirref.so not built")
+        ref = bridge.Reference()
     except Exception as e:  # noqa: BLE001
         print(json.dumps({"impl": "reference", "unavailable": f"FIR reference library unavailable: {e}"}))
         return 0
+    import numpy as np
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    ref.threads(os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    nb, y, sens = reference_inputs(w, ref)
+    counts = reference_counts(w, ref, nb)
+    prep_s = time.perf_counter() - t0
     nsub = w.osem.n_subsets
     budget = max(nsub, min(args.steps, 2 * nsub))
-    r = cpu_reference_run(w, budget)
+    iters = max(1, int(math.ceil(budget / nsub)))
+    r = cpu_reference_run(w, ref, y, sens, np.ones(w.vol.shape_zyx, np.float32), counts, iters)
     ms = 1000.0 * r["osem_s_per_iteration"] / nsub
     line = {
         "impl": "reference",
@@ -249,10 +287,10 @@ def reference_arm(args, rank):
         "scaling": "strong",
         "vs_baseline": None,
         "dtype": "f32 data, f64 geometry",
-        "data": "synthetic (seeded Poisson counts; uniform sensitivity)",
-        "config": {"workload": f"{w.name}: OSEM sub-iteration, 32 rings x 512 crystals, 300 mm FOV, "
-                               f"{w.n_lors} LORs, 200x200x64 @ 3 mm, {nsub} subsets, FWHM 4 mm",
-                   "osem_s_per_iteration": r["osem_s_per_iteration"]},
+        "data": "synthetic (seeded phantom, water attenuation, Poisson counts)",
+        "config": bench_config(w, world, nb),
+        "osem_s_per_iteration": r["osem_s_per_iteration"],
+        "input_prep_s": prep_s,
         "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -577,20 +615,19 @@ def main():
     if args.block:
         ctx.set_option(capi.FIR_OPT_BLOCK_SIZE, args.block)
 
-    # ---- data: attenuated, scaled, Poisson-sampled, precorrected (OSEM.cc:294-337)
+    # ---- data: attenuated, scaled, Poisson-sampled, precorrected (OSEM.cc:294-337);
+    # the two forward projections are bit-identical to FIR's, and the rest is
+    # host numpy, so the reference arm builds the same sinogram with FIR
     x_true = torch.from_numpy(workloads.activity(w)).to(dev)
     mu = torch.from_numpy(workloads.hounsfield(w)).to(dev)
     aux.hu_to_mu(w.vol, mu)
-    acf = torch.empty(nb, device=dev)
-    aux.forward_exp(w.vol, mu, w.proj, acf)
+    line_mu = torch.empty(nb, device=dev)
+    aux.forward(w.vol, mu, w.proj, line_mu)
     ax = torch.empty(nb, device=dev)
     aux.forward(w.vol, x_true, w.proj, ax)
-    expected = ax / acf
-    expected *= w.counts / float(expected.sum(dtype=torch.float64))
-    gen = torch.Generator(device=dev).manual_seed(w.seed)
-    y = torch.poisson(expected, generator=gen)
-    aux.proj_multiply(w.proj, y, acf)
-    del expected, ax, x_true
+    y_host = workloads.measured_sinogram(w, ax.cpu().numpy(), line_mu.cpu().numpy())
+    y = torch.from_numpy(y_host).to(dev)
+    del ax, x_true, line_mu, mu
     sens = torch.empty((nsub,) + tuple(w.vol.shape_zyx), device=dev)
     aux.sensitivity(w.proj, w.vol, sens, nsub)
     img = torch.ones(w.vol.shape_zyx, device=dev)
@@ -724,18 +761,10 @@ def main():
         "vs_baseline": None,
         "dtype": "f32 data, f64 geometry",
         "data": "synthetic (seeded phantom, water attenuation, Poisson counts)",
-        "config": {
-            "workload": f"{w.name}: OSEM sub-iteration, {w.proj.n_rings} rings x {w.proj.n_crystals_per_ring} "
-                        f"crystals, {w.proj.n_tang_coords} tangential bins, {nb} LORs, "
-                        f"{'x'.join(str(s) for s in w.vol.size)} @ {w.vol.voxel[0]} mm, {nsub} subsets, "
-                        f"FWHM {w.osem.fwhm_xyz[0]} mm",
-            "l2": "flushed (256 MB write) before every timed step, outside the step's events",
-            "osem_s_per_iteration": total_ms / args.steps * nsub / 1000.0,
-            "steps_per_subiteration": total_steps / args.steps,
-            "parallelism": f"views of each subset split over {world} GPUs, NCCL all-reduce of the backprojection"
-                           if world > 1 else "single GPU",
-            "wall_s_timed_loop": wall,
-        },
+        "config": bench_config(w, world, nb),
+        "osem_s_per_iteration": total_ms / args.steps * nsub / 1000.0,
+        "steps_per_subiteration": total_steps / args.steps,
+        "wall_s_timed_loop": wall,
         "gpu_launches": launches,
         "roofline": roofline,
         "clocks": {k2: v for k2, v in clocks.summary().items() if k2 != "samples"},
@@ -815,10 +844,13 @@ def main():
         prm1 = OSEMParams(n_iterations=1, n_subsets=nsub, convolution_interval=prm.convolution_interval,
                           fwhm_xyz=list(prm.fwhm_xyz), cut_radius=prm.cut_radius)
         ctx.osem(w.proj, y_h, w.vol, img_h, sens_h, prm1)  # stage buffers once (warm)
-        img_h.copy_(img)
-        t0 = time.perf_counter()
-        ctx.osem(w.proj, y_h, w.vol, img_h, sens_h, prm1)
-        dt = time.perf_counter() - t0
+        e2e_s = []
+        for _ in range(args.e2e_runs):
+            img_h.copy_(img)
+            t0 = time.perf_counter()
+            ctx.osem(w.proj, y_h, w.vol, img_h, sens_h, prm1)
+            e2e_s.append(time.perf_counter() - t0)
+        dt = statistics.median(e2e_s)
         h2d = (nb + sens.numel() + nvox) * 4
         result["e2e"] = {
             "value": e2e_steps / dt,
@@ -826,8 +858,9 @@ def main():
             "h2d_bytes_per_step": h2d // nsub,
             "d2h_bytes_per_step": (nvox * 4) // nsub,
             "call": "fir_osem with pinned host buffers, 1 iteration = "
-                    f"{nsub} steps, copies inside the timed region",
+                    f"{nsub} steps, copies inside the timed region; median of {len(e2e_s)} calls",
             "osem_s_per_iteration": dt,
+            "osem_s_per_iteration_all": e2e_s,
         }
 
     if args.batch_runs > 0 and world == 1:
@@ -839,7 +872,13 @@ def main():
 
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         try:
-            r = cpu_reference_run(w, nsub)
+            from oracle.bridge import Reference
+
+            ref = Reference()
+            ref.threads(os.cpu_count() or 1)
+            counts_ref = reference_counts(w, ref, nb)
+            r = cpu_reference_run(w, ref, y_host, sens.cpu().numpy(), np.ones(w.vol.shape_zyx, np.float32),
+                                  counts_ref, 1)
             result["cpu_baseline"] = {k2: r[k2] for k2 in ("value", "unit", "cores", "kind", "sample")}
             result["cpu_baseline"]["osem_s_per_iteration"] = r["osem_s_per_iteration"]
         except Exception as e:  # noqa: BLE001

@@ -116,6 +116,9 @@ _SIGS = {
                            C.c_void_p, C.c_void_p, C.POINTER(OsemParamsDesc), C.c_void_p, C.c_void_p]),
     "fir_osem_psf": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.c_void_p, C.c_void_p, C.POINTER(VolDesc),
                                C.c_void_p, C.c_void_p, C.POINTER(OsemParamsDesc), C.c_void_p, C.c_void_p]),
+    "fir_osem_reso_reco": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.c_void_p, C.c_void_p,
+                                     C.POINTER(VolDesc), C.c_void_p, C.c_void_p, C.c_int,
+                                     C.POINTER(OsemParamsDesc), C.c_void_p, C.c_void_p]),
     "fir_osem_weighted": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.POINTER(VolDesc), C.c_void_p, C.c_void_p, C.POINTER(OsemParamsDesc),
                                     C.c_void_p, C.c_void_p]),
@@ -427,6 +430,21 @@ class Context:
                   C.byref(vol_desc(vol, 1)), _ptr(img, writable=True, n=vol.n_voxels),
                   _ptr(sens, n=vol.n_voxels * params.n_subsets), C.byref(osem_desc(params)),
                   C.cast(cb, C.c_void_p) if cb is not None else None, None))
+
+    def osem_reso_reco(self, proj: ProjSpec, sino, vol: VolSpec, img, sens, params: OSEMParams,
+                       n_sens_frames: Optional[int] = None, bias=None) -> None:
+        """reconAlgos::OSEM_ResoReco as FIR runs it (``fir_osem_reso_reco``):
+        every frame of ``sens`` (``n_sens_frames``, default the number of
+        subsets) is filtered in place once, then every sub-iteration divides
+        the image by the subset's sensitivity frame and multiplies it by the
+        filtered backprojection of the unfiltered image's ratio."""
+        self._prep(sino, img, sens, bias)
+        nb = proj_geometry(proj)["n_bins"]
+        nf = int(params.n_subsets if n_sens_frames is None else n_sens_frames)
+        _check(lib().fir_osem_reso_reco(self._h, C.byref(proj_desc(proj)), _ptr(sino, n=nb), _ptr(bias, n=nb),
+                                        C.byref(vol_desc(vol, 1)), _ptr(img, writable=True, n=vol.n_voxels),
+                                        _ptr(sens, writable=True, n=vol.n_voxels * nf), nf,
+                                        C.byref(osem_desc(params)), None, None))
 
     def ratio_backprojection(self, proj: ProjSpec, sino, vol: VolSpec, img, bp, n_subsets: int = 1,
                              subset: int = 0, bias=None) -> None:

@@ -1145,6 +1145,79 @@ void osem_run(fir_ctx& c, const fir_proj_desc* proj, const float* sino, const fl
   finish(c, st);
 }
 
+// reconAlgos::OSEM_ResoReco as FIR runs it (reconAlgos.cc:203-367), with
+// every image on the device for the whole run.  Its order of operations:
+// the initial cut; every frame of the sensitivity volume filtered once, in
+// place (operations::convolve filters all frames, operations.cc:77-187;
+// reconAlgos.cc:232-236); then per sub-iteration the ratio backprojection of
+// the unfiltered image (:270-312), the filtered backprojection,
+// img <- img / sens_subset and img <- img * bp with the 1e-5 gates
+// (:315-326), the post-filter every convolution_interval sub-iterations and
+// the cut (:333-347).  FIR also filters a copy of the image every
+// sub-iteration (`blur`, :264-268 and :350-353) but never reads it; that work
+// has no effect and is not done.
+void osem_reso_reco_run(fir_ctx& c, const fir_proj_desc* proj, const float* sino, const float* bias,
+                        const fir_vol_desc* vol, float* img, float* sens, int n_sens_frames,
+                        const fir_osem_params* params, fir_osem_save_fn save, void* user)
+{
+  const ProjInfo p = check_proj(proj);
+  check_osem_params(params, p);
+  const VolInfo v = check_vol(vol);
+  check_frames(v, 1);
+  if (n_sens_frames < params->n_subsets)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "Invalid frame");
+  }
+  const Tables t = tables_of(c, p);
+  const Grid g = grid_of(c, v);
+  if (sino == nullptr || sens == nullptr || img == nullptr)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "sinogram, image and sensitivity must not be NULL");
+  }
+  Stager st(c);
+  const float* dsino = st.in(sino, p.g.n_bins);
+  const float* dbias = st.in(bias, p.g.n_bins);
+  float* dsens = st.inout(sens, v.nvox * n_sens_frames);
+  float* dimg = st.inout(img, v.nvox);
+  const size_t bytes = (size_t)v.nvox * sizeof(float);
+  float* bp = static_cast<float*>(c.bp.ensure(bytes));
+  cut_device(c, v, dimg, params->cut_radius, 1);
+  VolInfo frames = v;
+  frames.d.n_frames = n_sens_frames;
+  convolve_device(c, frames, dsens, params->fwhm_xyz, params->cut_radius);
+  const bool conv = params->convolution_interval > 0 && params->fwhm_xyz[0] > 0.0 &&
+                    params->fwhm_xyz[1] > 0.0 && params->fwhm_xyz[2] > 0.0;
+  const int nsub_total = params->n_iterations * params->n_subsets;
+  std::vector<float> host_copy;
+  for (int iter = 0; iter < params->n_iterations; ++iter)
+  {
+    for (int subset = 0; subset < params->n_subsets; ++subset)
+    {
+      const int subiter = iter * params->n_subsets + subset + 1;
+      cuda_ok(cudaMemsetAsync(bp, 0, bytes, c.stream), "cudaMemsetAsync");
+      const Sino s = sino_of(p, params->n_subsets, subset);
+      ratio_backproject(c, g, s, t, dimg, dsino, nullptr, dbias, bp, v.nvox);
+      convolve_device(c, v, bp, params->fwhm_xyz, params->cut_radius);
+      launch_em_update_image_first(v.nvox, dimg, bp, dsens + (size_t)subset * v.nvox, cfg_of(c));
+      after_launch(c);
+      if (conv && subiter % params->convolution_interval == 0)
+      {
+        convolve_device(c, v, dimg, params->fwhm_xyz, params->cut_radius);
+      }
+      cut_device(c, v, dimg, params->cut_radius, 1);
+      if (save != nullptr && params->save_interval > 0 && subiter % params->save_interval == 0 &&
+          subiter != nsub_total)
+      {
+        host_copy.resize((size_t)v.nvox);
+        cuda_ok(cudaMemcpyAsync(host_copy.data(), dimg, bytes, cudaMemcpyDeviceToHost, c.stream), "cudaMemcpyAsync");
+        cuda_ok(cudaStreamSynchronize(c.stream), "cudaStreamSynchronize");
+        save(user, subiter, host_copy.data());
+      }
+    }
+  }
+  finish(c, st);
+}
+
 }  // namespace fir::abi
 
 using namespace fir;
@@ -1665,6 +1738,15 @@ fir_status fir_osem_psf(fir_ctx* ctx, const fir_proj_desc* proj, const float* si
   });
 }
 
+fir_status fir_osem_reso_reco(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const float* bias,
+                              const fir_vol_desc* vol, float* img, float* sens, int n_sens_frames,
+                              const fir_osem_params* params, fir_osem_save_fn save, void* user)
+{
+  return guarded(__func__, [&] {
+    osem_reso_reco_run(check_ctx(ctx), proj, sino, bias, vol, img, sens, n_sens_frames, params, save, user);
+  });
+}
+
 fir_status fir_osem_weighted(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const float* mult,
                              const float* bias, const fir_vol_desc* vol, float* img, const float* sens,
                              const fir_osem_params* params, fir_osem_save_fn save, void* user)
@@ -1985,7 +2067,9 @@ fir_status fir_lor_paths(fir_ctx* ctx, const fir_proj_desc* proj, const fir_vol_
 // file-scope array below instead of from a context, and touches no host
 // memory, so it never allocates.  The array's device address is looked up
 // once per device with cudaGetSymbolAddress; the name itself is only a host
-// stand-in and is never passed to a kernel.
+// stand-in and is never passed to a kernel.  This file defines no kernel, so
+// under CUDA's lazy module loading (the default) the array is reserved when
+// that first lookup loads the module, not when the library is loaded.
 
 namespace
 {
@@ -2024,11 +2108,46 @@ unsigned char* noalloc_scratch()
   return static_cast<unsigned char*>(g_noalloc_address[device]);
 }
 
-void require_device(const void* p, const char* what)
+// p must be memory of the current device (where the scratch array and the
+// kernels live) or managed memory.
+void require_device(const void* p, const char* what, int device)
 {
-  if (p != nullptr && !is_device_ptr(p))
+  if (p == nullptr)
+  {
+    return;
+  }
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess)
+  {
+    cudaGetLastError();
+    a.type = cudaMemoryTypeUnregistered;
+  }
+  if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
   {
     fail(FIR_ERR_INVALID_ARGUMENT, what, " must be device memory for the no-allocation entry point");
+  }
+  if (a.type == cudaMemoryTypeDevice && a.device != device)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, what, " is memory of device ", a.device, ", the current device is ", device);
+  }
+}
+
+// The stream must belong to the current device (NULL: its default stream).
+void require_stream_on(cudaStream_t stream, int device)
+{
+  if (stream == nullptr)
+  {
+    return;
+  }
+  int d = -1;
+  if (cudaStreamGetDevice(stream, &d) != cudaSuccess)
+  {
+    cudaGetLastError();
+    fail(FIR_ERR_INVALID_ARGUMENT, "stream is not a valid CUDA stream");
+  }
+  if (d != device)
+  {
+    fail(FIR_ERR_INVALID_ARGUMENT, "stream belongs to device ", d, ", the current device is ", device);
   }
 }
 }  // namespace
@@ -2061,12 +2180,15 @@ extern "C" fir_status fir_osem_subiteration_noalloc(const fir_proj_desc* proj, c
     {
       fail(FIR_ERR_INVALID_ARGUMENT, "tables, sinogram, image and sensitivity must not be NULL");
     }
-    require_device(crystal_xy, "crystal_xy");
-    require_device(slice_z, "slice_z");
-    require_device(sino, "sino");
-    require_device(bias, "bias");
-    require_device(img, "img");
-    require_device(sens_frame, "sens_frame");
+    int device = 0;
+    cuda_ok(cudaGetDevice(&device), "cudaGetDevice");
+    require_device(crystal_xy, "crystal_xy", device);
+    require_device(slice_z, "slice_z", device);
+    require_device(sino, "sino", device);
+    require_device(bias, "bias", device);
+    require_device(img, "img", device);
+    require_device(sens_frame, "sens_frame", device);
+    require_stream_on(static_cast<cudaStream_t>(stream), device);
 
     // geometry as a context in the requested mode would build it
     fir_ctx geo;

@@ -86,11 +86,13 @@ void OSEM(const ProjData& inputProj, const ScannerData& scanner, VolData& output
   }
 }
 
-// FIR's resolution-modelling variant as FIR runs it (reconAlgos.cc:203-367),
-// including its order of operations: the sensitivity is filtered once, the
-// estimate used in the projection is the unfiltered image, the filtered
-// backprojection multiplies the image after the image (not the
-// backprojection) is divided by the sensitivity.
+// FIR's resolution-modelling variant as FIR runs it (reconAlgos.cc:203-367):
+// every frame of the sensitivity volume is filtered once, in place; each
+// sub-iteration projects the unfiltered image, filters the backprojection,
+// divides the image (not the backprojection) by the subset's sensitivity
+// frame and multiplies it by the filtered backprojection.  The whole loop
+// runs on the device (fir_osem_reso_reco); the volumes are copied in once
+// and out once.
 void OSEM_ResoReco(const ProjData& inputProj, const ScannerData& scanner, VolData& outputVol,
                    const std::string& outputVolFileName, const OSEMCoreParams& params, VolData& sensitivityMap,
                    const std::optional<ProjData>& biasProj)
@@ -99,48 +101,30 @@ void OSEM_ResoReco(const ProjData& inputProj, const ScannerData& scanner, VolDat
   scanner.checkProjData(inputProj);
   inputProj.checkNSubsets(params.nSubsets);
   checkSensitivity(sensitivityMap, outputVol, params.nSubsets);
+  if (biasProj && !(biasProj->getHeader() == inputProj.getHeader()))
+  {
+    error("Bias projection doesn't fit with the input projection");
+  }
   const fir_osem_params p = toParams(params);
-  const bool convolveFlag = params.convolutionInterval > 0 && params.fwhmXYZ[0] > 0.0 &&
-                            params.fwhmXYZ[1] > 0.0 && params.fwhmXYZ[2] > 0.0;
   fir_runtime::useScanner(scanner);
   const fir_vol_desc vd = fir_runtime::volDesc(outputVol, 1);
   const fir_proj_desc pd = fir_runtime::projDesc(inputProj);
-
-  VolData backProj(outputVol, VolData::ConstructionMode::INITIALIZE, 0.0);
-  operations::cutCircle(outputVol, params.cutRadius);
-  operations::convolve(sensitivityMap, params.fwhmXYZ, params.cutRadius);
-  VolData blur(outputVol, VolData::ConstructionMode::READ_DATA);
-  const int nSubiterations = params.nIterations * params.nSubsets;
-  for (int iter = 0; iter < params.nIterations; ++iter)
+  SaveTarget target{&outputVol, &outputVolFileName};
+  print("Iterations: ", params.nIterations, ", subsets: ", params.nSubsets);
+  fir_runtime::check(fir_osem_reso_reco(fir_runtime::context(), &pd, inputProj.getBins(),
+                                        biasProj ? biasProj->getBins() : nullptr, &vd, outputVol.getDataArray(),
+                                        sensitivityMap.getAllFrames(), sensitivityMap.getNFrames(), &p,
+                                        &saveSubiteration, &target),
+                     "OSEM_ResoReco");
+  // FIR's filter leaves the last frame active, the loop the last subset's
+  const bool filtered = params.fwhmXYZ[0] > 0.0 && params.fwhmXYZ[1] > 0.0 && params.fwhmXYZ[2] > 0.0;
+  if (params.nIterations > 0)
   {
-    print("Iteration ", iter + 1, " of ", params.nIterations);
-    for (int subset = 0; subset < params.nSubsets; ++subset)
-    {
-      const int subiter = iter * params.nSubsets + subset + 1;
-      operations::convolve(blur, params.fwhmXYZ, params.cutRadius);
-      fir_runtime::check(fir_ratio_backprojection(fir_runtime::context(), &pd, inputProj.getBins(),
-                                                  biasProj ? biasProj->getBins() : nullptr, &vd,
-                                                  outputVol.getDataArray(), backProj.getDataArray(),
-                                                  params.nSubsets, subset),
-                         "ratio backprojection");
-      operations::convolve(backProj, params.fwhmXYZ, params.cutRadius);
-      sensitivityMap.setActiveFrame(subset);
-      outputVol /= sensitivityMap;
-      outputVol *= backProj;
-      if (convolveFlag && subiter % params.convolutionInterval == 0)
-      {
-        operations::convolve(outputVol, params.fwhmXYZ, params.cutRadius);
-      }
-      operations::cutCircle(outputVol, params.cutRadius);
-      if (subiter != nSubiterations)
-      {
-        blur.assign(outputVol);
-      }
-      if (p.save_interval > 0 && subiter % p.save_interval == 0 && subiter != nSubiterations)
-      {
-        outputVol.write(outputVolFileName + "_subiter_" + std::to_string(subiter));
-      }
-    }
+    sensitivityMap.setActiveFrame(params.nSubsets - 1);
+  }
+  else if (filtered)
+  {
+    sensitivityMap.setActiveFrame(sensitivityMap.getNFrames() - 1);
   }
 }
 }  // namespace reconAlgos

@@ -36,6 +36,25 @@ __global__ void k_em_update(long long n, float* __restrict__ img, float* __restr
   bp[i] = q;
 }
 
+// The EM step of OSEM_ResoReco as FIR runs it (reconAlgos.cc:320-326):
+// img <- img/sens, then img <- img*bp, each with VolData's 1e-5 gates
+// (VolData.cc:305-343); the image, not the backprojection, is divided.
+__global__ void k_em_update_image_first(long long n, float* __restrict__ img, const float* __restrict__ bp,
+                                        const float* __restrict__ sens)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n)
+  {
+    return;
+  }
+  const float s = __ldg(sens + i);
+  const float b = __ldg(bp + i);
+  float x = img[i];
+  x = ((double)x > kEps && (double)s > kEps) ? __fdiv_rn(x, s) : 0.0f;
+  x = ((double)x > kEps && (double)b > kEps) ? __fmul_rn(x, b) : 0.0f;
+  img[i] = x;
+}
+
 __global__ void k_widen(long long n, const float* __restrict__ in, double* __restrict__ out)
 {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -313,6 +332,15 @@ void launch_em_update(long long n, float* img, float* bp, const float* sens, con
   if (n > 0)
   {
     k_em_update<<<blocks_for(n), kBlock, 0, cfg.stream>>>(n, img, bp, sens);
+  }
+}
+
+void launch_em_update_image_first(long long n, float* img, const float* bp, const float* sens,
+                                  const LaunchCfg& cfg)
+{
+  if (n > 0)
+  {
+    k_em_update_image_first<<<blocks_for(n), kBlock, 0, cfg.stream>>>(n, img, bp, sens);
   }
 }
 

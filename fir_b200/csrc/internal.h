@@ -80,6 +80,8 @@ struct Taps
   float w[2 * kMaxHalfTaps + 1];
 };
 void launch_em_update(long long n, float* img, float* bp, const float* sens, const LaunchCfg& cfg);
+void launch_em_update_image_first(long long n, float* img, const float* bp, const float* sens,
+                                  const LaunchCfg& cfg);
 // Exact widening of a float image to double for the projector gathers.
 void launch_widen(long long n, const float* in, double* out, const LaunchCfg& cfg);
 // Double copies of an [nz][ny][nx] image: out in the same layout, out_t as

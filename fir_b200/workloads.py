@@ -251,6 +251,35 @@ def poisson_counts(expected: np.ndarray, total: float, seed: int) -> np.ndarray:
     return np.random.default_rng(seed).poisson(lam).astype(np.float32)
 
 
+def measured_sinogram(w: Workload, ax: np.ndarray, line_mu: Optional[np.ndarray]) -> np.ndarray:
+    """Measured, attenuation-precorrected data of ``w`` from two forward
+    projections made by the caller's projector: ``ax`` = A x of the phantom
+    and ``line_mu`` = A mu of the attenuation map (FIR's HU-to-mu map), both
+    float32 in FIR's file order; ``line_mu=None`` means no attenuation.
+
+    The attenuation correction factors are ACF = exp(A mu) where A mu > 1e-5,
+    else 1 (ProjData::exponential, ProjData.cc:514-539; evaluated in double
+    and rounded once).  The expected counts A x / ACF are scaled to
+    ``w.counts``, Poisson-sampled with ``w.seed`` and multiplied by the
+    factors again, zero where either operand is <= 1e-5 (ProjData::operator*=,
+    ProjData.cc:481-512; the OSEM executable's precorrection, OSEM.cc:294-337).
+    Everything after the two projections runs here in numpy, so projectors
+    whose forward projections agree bit for bit (this library's and FIR's
+    own) give bit-identical data."""
+    ax = np.ascontiguousarray(ax, np.float32)
+    if line_mu is None:
+        acf = np.ones_like(ax)
+    else:
+        lm = np.ascontiguousarray(line_mu, np.float32)
+        acf = np.where(lm.astype(np.float64) > 1e-5, np.exp(lm.astype(np.float64)), 1.0).astype(np.float32)
+    expected = ax / acf
+    s = float(expected.sum(dtype=np.float64))
+    expected *= np.float32(w.counts / s if s > 0 else 0.0)
+    y = np.random.default_rng(w.seed).poisson(expected.astype(np.float64)).astype(np.float32)
+    keep = (y.astype(np.float64) > 1e-5) & (acf.astype(np.float64) > 1e-5)
+    return np.where(keep, y * acf, np.float32(0.0)).astype(np.float32)
+
+
 def measured_on_gpu(ctx, w: Workload, device, attenuation: bool = True):
     """Measured data of ``w`` made with the GPU projector of ``ctx`` (scanner
     and geometry already set): the phantom is forward-projected, divided by

@@ -12,6 +12,7 @@
  *   fir_osem               reconAlgos::OSEM                src_lib/reconAlgos.h:29-36, reconAlgos.cc:63-201
  *   fir_ratio_backprojection  the getLine/ratio/projectLineIntegral loop of OSEM and OSEM_ResoReco  src_lib/reconAlgos.cc:119-158, :273-312
  *   fir_osem_psf              reconAlgos::OSEM_ResoReco, corrected (PSF in the model)              src_lib/reconAlgos.cc:203-367
+ *   fir_osem_reso_reco        reconAlgos::OSEM_ResoReco as FIR runs it                           src_lib/reconAlgos.h:38-45, reconAlgos.cc:203-367
  *   fir_convolve           operations::convolve            src_lib/operations.h:7-10, operations.cc:11-192
  *   fir_cut_circle         operations::cutCircle           src_lib/operations.h:13-15, operations.cc:194-220
  *   fir_apply_mask         operations::applyMask           src_lib/operations.h:19, operations.cc:222-241
@@ -252,12 +253,18 @@ fir_status fir_osem_subiteration(fir_ctx* ctx, const fir_proj_desc* proj, const 
  * image, sensitivity frame, and the scanner tables crystal_xy = 2 *
  * n_crystals_per_ring doubles and slice_z = 2 * n_rings - 1 doubles, as
  * fir_scanner_tables returns them) must be device memory, and the work is
- * enqueued on `stream` (a cudaStream_t) without waiting.  Its scratch memory
- * is one array in the library's static device memory, 24 MiB on every GPU
- * that loads the library, held until the process exits; volumes of more than
- * 1048576 voxels (1 << 20) are rejected with FIR_ERR_INVALID_ARGUMENT.  The
- * first call on each device looks up the array's address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * enqueued on `stream` (a cudaStream_t) without waiting.  Pointers and
+ * stream must belong to the current device.  Its scratch memory is one
+ * array in the library's static device memory, 24 MiB per device, held
+ * until the process exits; volumes of more than 1048576 voxels (1 << 20) are
+ * rejected with FIR_ERR_INVALID_ARGUMENT.  The first call on each device
+ * looks up the array's address (cudaGetSymbolAddress).  Under CUDA's lazy
+ * module loading (the default since CUDA 12.2) that lookup is what reserves
+ * the 24 MiB on the device, so a caller that fixes its memory budget at
+ * start-up should make one call (or one warm-up call on a small volume) on
+ * each device before it reserves its budget, or run with
+ * CUDA_MODULE_LOADING=EAGER, which reserves the array when the library is
+ * loaded.  Make that first call before any stream capture.
  * All calls on a device share the one array, so calls that can overlap on
  * the GPU (different streams, no ordering between them) race and corrupt
  * each other; order them on one stream.  The accumulator is cleared by each
@@ -301,6 +308,24 @@ fir_status fir_osem(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, 
 fir_status fir_osem_psf(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const float* bias,
                         const fir_vol_desc* vol, float* img, const float* sens, const fir_osem_params* params,
                         fir_osem_save_fn save, void* user);
+
+/* reconAlgos::OSEM_ResoReco exactly as FIR runs it (reconAlgos.cc:203-367),
+ * with the images kept on the device for the whole run:
+ * - the initial cut, then every one of the n_sens_frames (>= n_subsets)
+ *   frames of sens is filtered in place, once (FIR's operations::convolve
+ *   filters all frames of the sensitivity volume);
+ * - per sub-iteration: the ratio backprojection of the unfiltered image
+ *   (as fir_ratio_backprojection), the backprojection filtered, then
+ *   img <- img / sens[subset] and img <- img * bp with the 1e-5 gates of
+ *   VolData's operators, the post-filter every convolution_interval
+ *   sub-iterations, and the cut.
+ * These are FIR's own steps, including the two that fir_osem_psf corrects
+ * (the projection of the unfiltered image, reconAlgos.cc:296, and the
+ * division of the image by the sensitivity, :323).  sens is read and
+ * written (host buffers are copied back).  save may be NULL. */
+fir_status fir_osem_reso_reco(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino, const float* bias,
+                              const fir_vol_desc* vol, float* img, float* sens, int n_sens_frames,
+                              const fir_osem_params* params, fir_osem_save_fn save, void* user);
 
 /* OSEM with the ordinary-Poisson system model: the mean of bin i is
  * m_i (A x)_i + bias_i, with m the per-bin multiplicative factors

@@ -29,22 +29,29 @@ RESTATED_SO = os.path.join(HERE, "libfir_oracle.so")
 REF_BIN = os.path.join(HERE, "_ref")
 DROPIN_BIN = os.path.join(HERE, "_ref", "dropin")
 REF_SO = os.path.join(HERE, "_ref", "libfirref.so")
-REF_SOURCES = os.environ.get("FIR_REFERENCE_SRC", "/root/reference")
+# FIR checkout whose sources build the reference oracle; the build is
+# skipped, with a message, when it is not given.
+REF_SOURCES = os.environ.get("FIR_REFERENCE_SRC", "")
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 
 
-def build(reference: bool = True) -> None:
+def build(reference: bool = True, source: Optional[str] = None) -> None:
     """Builds the restatement, and the reference (plus FIR's executables
-    compiled against the drop-in layer) when FIR's sources exist."""
+    compiled against the drop-in layer) from the FIR checkout ``source``
+    (default: $FIR_REFERENCE_SRC).  Without a checkout only the restatement
+    is built; the reference oracle is then whatever oracle/_ref holds."""
     targets = ["restated"]
-    if reference and os.path.isdir(os.path.join(REF_SOURCES, "src_lib")):
+    src = source or REF_SOURCES
+    if reference and src and os.path.isdir(os.path.join(src, "src_lib")):
         targets.append("reference")
         if os.path.exists(os.path.join(ROOT, "fir_b200", "lib", "libfir.so")):
             targets.append("dropin")
-    subprocess.run(["make", "-s", "-C", HERE, f"REF={REF_SOURCES}", "-j8"] + targets, check=True)
+    elif reference:
+        print("oracle: no FIR checkout given (FIR_REFERENCE_SRC); the reference oracle is not rebuilt")
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={src}", "-j8"] + targets, check=True)
 
 
 def reference_available() -> bool:
@@ -135,6 +142,8 @@ class Restated:
         L.fo_osem.argtypes = [C.POINTER(FoProj), _f32p, C.c_void_p, C.POINTER(FoVol), C.c_int, _f64p, _f64p,
                               _f32p, _f32p, C.POINTER(FoOsem)]
         L.fo_osem_psf.argtypes = L.fo_osem.argtypes
+        L.fo_osem_reso_reco.argtypes = [C.POINTER(FoProj), _f32p, C.c_void_p, C.POINTER(FoVol), C.c_int, _f64p,
+                                        _f64p, _f32p, _f32p, C.c_int, C.POINTER(FoOsem)]
         L.fo_osem_weighted.argtypes = [C.POINTER(FoProj), _f32p, _f32p, C.c_void_p, C.POINTER(FoVol), C.c_int,
                                        _f64p, _f64p, _f32p, _f32p, C.POINTER(FoOsem)]
         L.fo_bin_coordinates.argtypes = [C.POINTER(FoProj)] + [C.c_int] * 4 + [C.POINTER(C.c_int)] * 4
@@ -260,6 +269,21 @@ class Restated:
            np.ascontiguousarray(sens, np.float32).ravel(), C.byref(o))
         return img.reshape(v.shape_zyx)
 
+    def osem_reso_reco(self, s, p, v, sino, img, sens, prm: OSEMParams, bias=None, truncate: bool = True):
+        """reconAlgos::OSEM_ResoReco as FIR runs it; returns (image, sens),
+        every frame of sens filtered in place."""
+        f = self.proj(p)
+        xy, z = self.scanner_tables(s)
+        img = np.ascontiguousarray(img, np.float32).copy().ravel()
+        sens = np.ascontiguousarray(sens, np.float32).copy().ravel()
+        o = FoOsem(prm.n_iterations, prm.n_subsets, prm.convolution_interval, prm.cut_radius)
+        o.fwhm[:] = [float(x) for x in prm.fwhm_xyz]
+        bias_arr = None if bias is None else np.ascontiguousarray(bias, np.float32)
+        bptr = None if bias_arr is None else bias_arr.ctypes.data_as(C.c_void_p)
+        self.L.fo_osem_reso_reco(C.byref(f), np.ascontiguousarray(sino, np.float32), bptr, C.byref(fo_vol(v)),
+                                 int(truncate), xy, z, img, sens, sens.size // v.n_voxels, C.byref(o))
+        return img.reshape(v.shape_zyx), sens
+
     def bin_coordinates(self, p: ProjSpec, pairs):
         """[n, 5]: flag, seg, view, axial, tang of each (ring1, crystal1,
         ring2, crystal2) pair (zeros where the flag is 0)."""
@@ -351,6 +375,8 @@ class Reference:
         L.ref_sensitivity.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(RefVol), C.c_int, _f32p]
         L.ref_osem.argtypes = [C.c_char_p, C.c_char_p, _f32p, C.c_void_p, C.POINTER(RefVol), _f32p, _f32p,
                                C.c_int, C.c_int, C.c_float, C.c_int, _f32p, C.c_int, C.c_char_p]
+        L.ref_osem_reso_reco.argtypes = [C.c_char_p, C.c_char_p, _f32p, C.c_void_p, C.POINTER(RefVol), _f32p,
+                                         _f32p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _f32p, C.c_char_p]
         L.ref_convolve.argtypes = [C.POINTER(RefVol), _f32p, _f32p, C.c_float]
         L.ref_cut_circle.argtypes = [C.POINTER(RefVol), _f32p, C.c_float]
         L.ref_apply_mask.argtypes = [C.POINTER(RefVol), _f32p, _f32p]
@@ -456,6 +482,22 @@ class Reference:
                                     prm.n_subsets, prm.cut_radius, prm.convolution_interval,
                                     np.asarray(prm.fwhm_xyz, np.float32), prm.save_interval, out_name))
         return img.reshape(v.shape_zyx)
+
+    def osem_reso_reco(self, s, p, v: VolSpec, sino, img, sens, prm: OSEMParams, bias=None):
+        """FIR's reconAlgos::OSEM_ResoReco; returns (image, sens), FIR having
+        filtered every frame of the sensitivity in place."""
+        sp, hp = self._files(s, p)
+        img = np.ascontiguousarray(img, np.float32).copy().ravel()
+        sens = np.ascontiguousarray(sens, np.float32).copy().ravel()
+        bias_arr = None if bias is None else np.ascontiguousarray(bias, np.float32)
+        bptr = None if bias_arr is None else bias_arr.ctypes.data_as(C.c_void_p)
+        out_name = os.path.join(self.tmp, f"reso{self._n}").encode()
+        self._check(self.L.ref_osem_reso_reco(sp, hp, np.ascontiguousarray(sino, np.float32), bptr,
+                                              C.byref(ref_vol(v)), img, sens, sens.size // v.n_voxels,
+                                              prm.n_iterations, prm.n_subsets, prm.cut_radius,
+                                              prm.convolution_interval, np.asarray(prm.fwhm_xyz, np.float32),
+                                              out_name))
+        return img.reshape(v.shape_zyx), sens
 
     def convolve(self, v: VolSpec, img, fwhm, cut_radius=0.0):
         out = np.ascontiguousarray(img, np.float32).copy()

@@ -715,6 +715,81 @@ void fo_osem_psf(const fo_proj* p, const float* sino, const float* bias, const f
   osem_loop(p, sino, NULL, bias, v, truncate, xy, z, img, sens, prm, psf);
 }
 
+/* reconAlgos::OSEM_ResoReco as FIR runs it (reconAlgos.cc:203-367): the
+ * initial cut (:229); all n_sens_frames frames of the sensitivity filtered in
+ * place (:232-236; operations::convolve filters every frame,
+ * operations.cc:77-187); per sub-iteration the ratio backprojection of
+ * the unfiltered image (:270-312), the backprojection filtered (:315-319),
+ * img /= sens[subset] and img *= bp with VolData's gates (:321-326;
+ * VolData.cc:305-343), the post-filter (:333-341) and the cut (:344).  The
+ * filtered copy `blur` (:239, :264-268, :350-353) is never read and is left
+ * out. */
+void fo_osem_reso_reco(const fo_proj* p, const float* sino, const float* bias, const fo_vol* v, int truncate,
+                       const double* xy, const double* z, float* img, float* sens, int n_sens_frames,
+                       const fo_osem_params* prm)
+{
+  fo_grid g;
+  fo_grid_init(&g, v, truncate);
+  const long long nvox = (long long)v->nx * v->ny * v->nz;
+  float* bp = (float*)calloc((size_t)nvox, sizeof(float));
+  const int cap = v->nx + v->ny + v->nz + 2;
+  int* co = (int*)malloc(sizeof(int) * (size_t)cap);
+  double* le = (double*)malloc(sizeof(double) * (size_t)cap);
+  const int conv = prm->convolution_interval > 0 && prm->fwhm[0] > 0.0 && prm->fwhm[1] > 0.0 &&
+                   prm->fwhm[2] > 0.0;
+  const int nsub = prm->n_subsets, vps = p->n_views / nsub;
+  fo_cut_circle(v, img, prm->cut_radius);
+  for (int f = 0; f < n_sens_frames; ++f) fo_convolve(v, sens + nvox * f, prm->fwhm, prm->cut_radius);
+  for (int iter = 0; iter < prm->n_iterations; ++iter)
+    for (int subset = 0; subset < nsub; ++subset)
+    {
+      const int subiter = iter * nsub + subset + 1;
+      memset(bp, 0, sizeof(float) * (size_t)nvox);
+      for (int seg = -p->seg_offset; seg <= p->seg_offset; ++seg)
+      {
+        const int nax = p->n_axial[seg + p->seg_offset];
+        const long long bpv = (long long)nax * p->n_tang_coords;
+        const long long base = seg_base(p, seg);
+        for (int sv = 0; sv < vps; ++sv)
+        {
+          const int view = sv * nsub + subset;
+          for (int ax = 0; ax < nax; ++ax)
+            for (int ti = 0; ti < p->n_tang_coords; ++ti)
+            {
+              const long long bin = base + view * bpv + (long long)ax * p->n_tang_coords + ti;
+              double e[6];
+              lor_ends(p, xy, z, seg, view, ax, ti - p->tang_offset, e);
+              int n;
+              const int crosses = fo_siddon(&g, e[0], e[1], e[2], e[3], e[4], e[5], co, le, cap, &n);
+              float line = 0.0f;
+              if (crosses)
+                for (int k = 0; k < n; ++k) line = (float)((double)line + le[k] * (double)img[co[k]]);
+              if (bias) line += bias[bin];
+              if ((double)line > FO_EPS)
+              {
+                const float ratio = sino[bin] / line;
+                for (int k = 0; k < n; ++k) bp[co[k]] = (float)((double)bp[co[k]] + le[k] * (double)ratio);
+              }
+            }
+        }
+      }
+      fo_convolve(v, bp, prm->fwhm, prm->cut_radius);
+      const float* sf = sens + nvox * subset;
+      for (long long i = 0; i < nvox; ++i)
+      {
+        float x = img[i];
+        x = ((double)x > FO_EPS && (double)sf[i] > FO_EPS) ? x / sf[i] : 0.0f;
+        x = ((double)x > FO_EPS && (double)bp[i] > FO_EPS) ? x * bp[i] : 0.0f;
+        img[i] = x;
+      }
+      if (conv && subiter % prm->convolution_interval == 0) fo_convolve(v, img, prm->fwhm, prm->cut_radius);
+      fo_cut_circle(v, img, prm->cut_radius);
+    }
+  free(bp);
+  free(co);
+  free(le);
+}
+
 /* ProjData::getBinCoordinates (ProjData.cc:342-479): the sinogram bin of the
  * LOR between (ring1, crystal1) and (ring2, crystal2), in integer arithmetic
  * with C's truncating division.  Returns 0 when the LOR lies outside the

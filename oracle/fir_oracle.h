@@ -104,6 +104,14 @@ void fo_osem_psf(const fo_proj* p, const float* sino, const float* bias, const f
                  int truncate, const double* xy, const double* z, float* img,
                  const float* sens, const fo_osem_params* prm);
 
+/* reconAlgos::OSEM_ResoReco exactly as FIR runs it (reconAlgos.cc:203-367):
+ * every frame of sens (n_sens_frames >= n_subsets) filtered in place once,
+ * the unfiltered image projected, img /= sens[subset], img *= the filtered
+ * backprojection. */
+void fo_osem_reso_reco(const fo_proj* p, const float* sino, const float* bias, const fo_vol* v,
+                       int truncate, const double* xy, const double* z, float* img, float* sens,
+                       int n_sens_frames, const fo_osem_params* prm);
+
 void fo_em_update(long long n, float* img, float* bp, const float* sens);
 
 /* OSEM with per-bin multiplicative factors m (ordinary-Poisson model):

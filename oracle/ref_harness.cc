@@ -436,6 +436,61 @@ int ref_osem(
     });
 }
 
+// reconAlgos::OSEM_ResoReco (reconAlgos.cc:203-367) on FIR's own code; the
+// sensitivity volume of nSensFrames frames is copied back (FIR filters it in
+// place).
+int ref_osem_reso_reco(
+  const char* scannerFile,
+  const char* projHeader,
+  const float* sino,
+  const float* bias,
+  const ref_vol* v,
+  float* img,
+  float* sens,
+  int nSensFrames,
+  int nIterations,
+  int nSubsets,
+  float cutRadius,
+  int convolutionInterval,
+  const float* fwhmXYZ,
+  const char* outName)
+{
+  return guarded(
+    [&]
+    {
+      ProjData proj(projHeader, ProjData::ConstructionMode::ALLOCATE);
+      projIn(proj, sino);
+      std::optional<ProjData> biasProj;
+      if (bias != nullptr)
+      {
+        biasProj.emplace(proj, ProjData::ConstructionMode::ALLOCATE);
+        projIn(*biasProj, bias);
+      }
+      ScannerData scanner(scannerFile);
+      VolData vol(toHeader(v, 1));
+      copyIn(vol, img);
+      VolData sensVol(toHeader(v, nSensFrames));
+      copyIn(sensVol, sens);
+      OSEMCoreParams params;
+      params.nIterations = nIterations;
+      params.nSubsets = nSubsets;
+      params.saveInterval = 0;
+      params.cutRadius = cutRadius;
+      params.convolutionInterval = convolutionInterval;
+      params.fwhmXYZ = {fwhmXYZ[0], fwhmXYZ[1], fwhmXYZ[2]};
+      reconAlgos::OSEM_ResoReco(
+        proj,
+        scanner,
+        vol,
+        outName ? std::string(outName) : std::string("osem_reso"),
+        params,
+        sensVol,
+        biasProj);
+      copyOut(vol, img);
+      copyOut(sensVol, sens);
+    });
+}
+
 int ref_convolve(const ref_vol* v, float* img, const float* fwhmXYZ, float cutRadius)
 {
   return guarded(

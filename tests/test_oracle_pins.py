@@ -182,6 +182,29 @@ def test_oracle_bit_identical_to_fir_small_workload(restated, reference):
     np.testing.assert_array_equal(o1, o2)
 
 
+@pytest.mark.parametrize("extra_frames,cut,interval", [(1, 110.0, 2), (0, 0.0, 1)])
+def test_oracle_reso_reco_bit_identical_to_fir(restated, reference, extra_frames, cut, interval):
+    """OSEM_ResoReco as FIR runs it (reconAlgos.cc:203-367): the restatement
+    against FIR's own function on one thread, image and sensitivity (every
+    frame of which FIR filters in place) bit for bit."""
+    w = workloads.small()
+    reference.threads(1)
+    x = workloads.activity(w)
+    nb = reference.proj_geometry(w.proj)["n_bins"]
+    s1 = restated.forward(w.scanner, w.proj, w.vol, x)
+    y = workloads.poisson_counts(s1, w.counts, 4)
+    sens4 = restated.sensitivity(w.scanner, w.proj, w.vol, 4).reshape(4, -1)
+    sens = np.concatenate([sens4] + [sens4.sum(axis=0, keepdims=True)] * extra_frames)
+    bias = np.full(nb, 0.02, np.float32)
+    prm = OSEMParams(n_iterations=2, n_subsets=4, convolution_interval=interval, fwhm_xyz=[4.0, 4.0, 4.0],
+                     cut_radius=cut)
+    i1, sn1 = restated.osem_reso_reco(w.scanner, w.proj, w.vol, y, np.ones_like(x), sens, prm, bias=bias)
+    i2, sn2 = reference.osem_reso_reco(w.scanner, w.proj, w.vol, y, np.ones_like(x), sens, prm, bias=bias)
+    np.testing.assert_array_equal(sn1, sn2)
+    np.testing.assert_array_equal(i1, i2)
+    assert not np.array_equal(sn1, sens.ravel()) and float(i1.max()) > 0
+
+
 def test_oracle_span3_and_lor_tables(restated, reference):
     for p in (ProjSpec(5, 32, 3, 8, 3), ProjSpec(9, 64, 5, 0, 3), ProjSpec(8, 128, 15, 43, 1)):
         nb = reference.proj_geometry(p)["n_bins"]
