@@ -128,6 +128,9 @@ _SIGS = {
                                                 C.c_void_p]),
     "fir_ratio_backprojection": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.c_void_p, C.c_void_p,
                                            C.POINTER(VolDesc), C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
+    "fir_ratio_backprojection_shard": (C.c_int, [C.c_void_p, C.POINTER(ProjDesc), C.c_void_p, C.c_void_p,
+                                                 C.POINTER(VolDesc), C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                                 C.c_int, C.c_int]),
     "fir_em_update": (C.c_int, [C.c_void_p, C.POINTER(VolDesc), C.c_void_p, C.c_void_p, C.c_void_p]),
     "fir_convolve": (C.c_int, [C.c_void_p, C.POINTER(VolDesc), C.c_void_p, C.POINTER(C.c_float), C.c_float]),
     "fir_cut_circle": (C.c_int, [C.c_void_p, C.POINTER(VolDesc), C.c_void_p, C.c_float]),
@@ -447,13 +450,18 @@ class Context:
                                         C.byref(osem_desc(params)), None, None))
 
     def ratio_backprojection(self, proj: ProjSpec, sino, vol: VolSpec, img, bp, n_subsets: int = 1,
-                             subset: int = 0, bias=None) -> None:
-        """bp <- backprojection of sino / (projection of img + bias) over one subset."""
+                             subset: int = 0, bias=None, n_shards: int = 1, shard: int = 0) -> None:
+        """bp <- backprojection of sino / (projection of img + bias) over one
+        subset, or over shard ``shard`` of ``n_shards`` of its views (the
+        subset's k-th view with k % n_shards == shard)."""
         self._prep(sino, img, bp, bias)
         nb = proj_geometry(proj)["n_bins"]
-        _check(lib().fir_ratio_backprojection(self._h, C.byref(proj_desc(proj)), _ptr(sino, n=nb), _ptr(bias, n=nb),
-                                              C.byref(vol_desc(vol, 1)), _ptr(img, n=vol.n_voxels),
-                                              _ptr(bp, writable=True, n=vol.n_voxels), int(n_subsets), int(subset)))
+        args = (self._h, C.byref(proj_desc(proj)), _ptr(sino, n=nb), _ptr(bias, n=nb), C.byref(vol_desc(vol, 1)),
+                _ptr(img, n=vol.n_voxels), _ptr(bp, writable=True, n=vol.n_voxels), int(n_subsets), int(subset))
+        if n_shards == 1:
+            _check(lib().fir_ratio_backprojection(*args))
+        else:
+            _check(lib().fir_ratio_backprojection_shard(*args, int(n_shards), int(shard)))
 
     # -- image / sinogram operations
     def em_update(self, vol: VolSpec, img, bp, sens_frame) -> None:

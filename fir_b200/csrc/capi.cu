@@ -664,7 +664,13 @@ Grid grid_of(const fir_ctx& c, const VolInfo& v)
   return g;
 }
 
-Sino sino_of(const ProjInfo& p, int n_subsets, int subset)
+// Enumeration of the views v = offset + stride * j < n_views, segment by
+// segment in FIR's order.  With stride = n_subsets dividing the number of
+// views this is FIR's subset `offset` (LORCache.cc:49-51, 115-133), and the
+// enumeration bases are the same for every offset.  A stride that does not
+// divide the number of views (a subset's views shared unevenly between
+// ranks) gives the first offsets one view more than the last.
+Sino sino_of_views(const ProjInfo& p, int stride, int offset)
 {
   Sino s;
   std::memset(&s, 0, sizeof(s));
@@ -677,21 +683,25 @@ Sino sino_of(const ProjInfo& p, int n_subsets, int subset)
   s.tang_offset = p.g.tang_offset;
   s.n_views = p.g.n_views;
   s.n_tang = p.g.n_tang_coords;
-  s.n_subsets = n_subsets;
-  s.subset = subset;
-  long long base = 0;
+  s.n_subsets = stride;
+  s.subset = offset;
+  const long long views = offset < s.n_views ? (s.n_views - offset + stride - 1) / stride : 0;
+  long long base = 0, ebase = 0;
   for (int k = 0; k < s.n_segments; ++k)
   {
     s.seg_base[k] = (int)base;
-    s.enum_base[k] = (int)(base / n_subsets);
+    s.enum_base[k] = (int)ebase;
     s.n_axial[k] = p.n_axial[k];
     base += (long long)p.n_axial[k] * s.n_views * s.n_tang;
+    ebase += (long long)p.n_axial[k] * views * s.n_tang;
   }
   s.seg_base[s.n_segments] = (int)base;
-  s.enum_base[s.n_segments] = (int)(base / n_subsets);
-  s.n_enum = (int)(base / n_subsets);
+  s.enum_base[s.n_segments] = (int)ebase;
+  s.n_enum = (int)ebase;
   return s;
 }
+
+Sino sino_of(const ProjInfo& p, int n_subsets, int subset) { return sino_of_views(p, n_subsets, subset); }
 
 // Page-locked host memory (cudaHostAlloc / cudaHostRegister), which the copy
 // engines read asynchronously.
@@ -1787,6 +1797,46 @@ fir_status fir_ratio_backprojection(fir_ctx* ctx, const fir_proj_desc* proj, con
     cuda_ok(cudaMemsetAsync(dbp, 0, (size_t)v.nvox * sizeof(float), c.stream), "cudaMemsetAsync");
     const Sino s = sino_of(p, n_subsets, subset);
     ratio_backproject(c, g, s, t, dimg, dsino, nullptr, dbias, dbp, v.nvox);
+    finish(c, st);
+  });
+}
+
+fir_status fir_ratio_backprojection_shard(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino,
+                                          const float* bias, const fir_vol_desc* vol, const float* img, float* bp,
+                                          int n_subsets, int subset, int n_shards, int shard)
+{
+  return guarded(__func__, [&] {
+    fir_ctx& c = check_ctx(ctx);
+    const ProjInfo p = check_proj(proj);
+    check_subsets(p, n_subsets);
+    if (subset < 0 || subset >= n_subsets)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "subset ", subset, " out of range [0, ", n_subsets, ")");
+    }
+    if (n_shards <= 0 || shard < 0 || shard >= n_shards || (long long)n_subsets * n_shards > (1LL << 30))
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "shard ", shard, " of ", n_shards, " is not valid");
+    }
+    const VolInfo v = check_vol(vol);
+    check_frames(v, 1);
+    const Tables t = tables_of(c, p);
+    const Grid g = grid_of(c, v);
+    if (sino == nullptr || img == nullptr || bp == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "sinogram, image and backprojection must not be NULL");
+    }
+    Stager st(c);
+    const float* dsino = st.in(sino, p.g.n_bins);
+    const float* dbias = st.in(bias, p.g.n_bins);
+    const float* dimg = st.in(img, v.nvox);
+    float* dbp = st.out(bp, v.nvox);
+    cuda_ok(cudaMemsetAsync(dbp, 0, (size_t)v.nvox * sizeof(float), c.stream), "cudaMemsetAsync");
+    // the subset's views subset + n_subsets * k with k % n_shards == shard
+    const Sino s = sino_of_views(p, n_subsets * n_shards, subset + n_subsets * shard);
+    if (s.n_enum > 0)
+    {
+      ratio_backproject(c, g, s, t, dimg, dsino, nullptr, dbias, dbp, v.nvox);
+    }
     finish(c, st);
   });
 }

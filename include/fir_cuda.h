@@ -285,6 +285,20 @@ fir_status fir_ratio_backprojection(fir_ctx* ctx, const fir_proj_desc* proj, con
                                     const float* bias, const fir_vol_desc* vol, const float* img,
                                     float* bp, int n_subsets, int subset);
 
+/* One rank's share of fir_ratio_backprojection when a subset's views are
+ * split between n_shards ranks (or GPUs): bp is zeroed, then the views
+ * subset + n_subsets * k of the subset with k % n_shards == shard are
+ * projected, and the ratio backprojected, exactly as fir_ratio_backprojection
+ * does for the whole subset.  The shares of shards 0..n_shards-1 partition
+ * the subset for any n_shards (the first shards hold one view more when
+ * n_shards does not divide the subset's views), so the sum of their bp is
+ * the subset's backprojection up to the order of the float additions.
+ * Counterpart: the subset loop of reconAlgos.cc:119-158, split across
+ * processes (FIR has one process). */
+fir_status fir_ratio_backprojection_shard(fir_ctx* ctx, const fir_proj_desc* proj, const float* sino,
+                                          const float* bias, const fir_vol_desc* vol, const float* img, float* bp,
+                                          int n_subsets, int subset, int n_shards, int shard);
+
 /* Called by fir_osem after sub-iteration `subiter` when params->save_interval
  * asks for an intermediate image; img is a host copy (nx*ny*nz floats). */
 typedef void (*fir_osem_save_fn)(void* user, int subiter, const float* img);

@@ -37,7 +37,7 @@ class OracleBackend:
         self.R = Restated()
         self.w = w
 
-    def ratio_backprojection(self, proj, sino, vol, img, bp, n_subsets, subset, bias=None):
+    def ratio_backprojection(self, proj, sino, vol, img, bp, n_subsets, subset, bias=None, n_shards=1, shard=0):
         w = self.w
         line = self.R.forward(w.scanner, proj, vol, img.numpy())
         if bias is not None:
@@ -46,9 +46,12 @@ class OracleBackend:
         ok = line.astype(np.float64) > EPS
         ratio = np.zeros_like(line)
         ratio[ok] = y[ok] / line[ok]
-        frames = self.R.backward(w.scanner, proj, vol, ratio, n_subsets)
-        nz = vol.size[2]
-        bp.copy_(torch.from_numpy(frames[subset * nz:(subset + 1) * nz].copy()))
+        # bins of the other views backproject a ratio of exactly 0
+        views = view_of_bins(self.R, proj)
+        k = views // n_subsets
+        ratio[~((views % n_subsets == subset) & (k % n_shards == shard))] = 0.0
+        frames = self.R.backward(w.scanner, proj, vol, ratio, 1)
+        bp.copy_(torch.from_numpy(frames.copy()))
 
     def em_update(self, vol, img, bp, sens):
         a, b = self.R.em_update(img.numpy(), bp.numpy(), sens.numpy())
@@ -60,6 +63,15 @@ class OracleBackend:
 
     def cut_circle(self, vol, img, cut):
         img.copy_(torch.from_numpy(self.R.cut_circle(vol, img.numpy(), cut)))
+
+
+def view_of_bins(R, proj):
+    """View index of every bin, FIR's file order (segments of [view][axial][tang])."""
+    f = R.proj(proj)
+    parts = []
+    for k in range(proj.n_segments):
+        parts.append(np.repeat(np.arange(f.n_views), f.n_axial[k] * f.n_tang_coords))
+    return np.concatenate(parts)
 
 
 def free_port():
@@ -75,7 +87,7 @@ def problem():
     return w, prm
 
 
-def _rank_main(rank, world, port, outdir, fail_rank):
+def _rank_main(rank, world, port, outdir, fail_rank, exchange="all_reduce"):
     import sys
 
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
@@ -93,7 +105,8 @@ def _rank_main(rank, world, port, outdir, fail_rank):
         if rank == fail_rank:
             raise RuntimeError("injected failure before the first exchange")
         img = torch.ones(w.vol.shape_zyx, dtype=torch.float32)
-        ShardedOSEM(OracleBackend(w), w.proj, w.vol, prm).run(torch.from_numpy(y), img, torch.from_numpy(sens))
+        ShardedOSEM(OracleBackend(w), w.proj, w.vol, prm, exchange=exchange).run(torch.from_numpy(y), img,
+                                                                                 torch.from_numpy(sens))
         np.save(os.path.join(outdir, f"img{rank}.npy"), img.numpy())
     except Exception as e:  # noqa: BLE001
         with open(os.path.join(outdir, f"err{rank}.txt"), "w") as f:
@@ -106,11 +119,12 @@ def _rank_main(rank, world, port, outdir, fail_rank):
             pass
 
 
-def _launch(world, fail_rank=-1, deadline=240):
+def _launch(world, fail_rank=-1, deadline=240, exchange="all_reduce"):
     outdir = tempfile.mkdtemp(prefix="firdist_")
     ctx = mp.get_context("spawn")
     port = free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, world, port, outdir, fail_rank)) for r in range(world)]
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, outdir, fail_rank, exchange))
+             for r in range(world)]
     for p in procs:
         p.start()
     for p in procs:
@@ -122,13 +136,18 @@ def _launch(world, fail_rank=-1, deadline=240):
     return outdir, [p.exitcode for p in procs], hung
 
 
-def test_sharded_osem_matches_single_process_oracle(restated):
-    outdir, codes, hung = _launch(2)
-    assert not hung and codes == [0, 0], open(os.path.join(outdir, "err0.txt")).read() \
-        if os.path.exists(os.path.join(outdir, "err0.txt")) else codes
+@pytest.mark.parametrize("world,exchange", [(2, "all_reduce"), (3, "all_reduce"), (2, "reduce_scatter"),
+                                            (3, "reduce_scatter")])
+def test_sharded_osem_matches_single_process_oracle(restated, world, exchange):
+    """World 3 splits each subset's 8 views 3 + 3 + 2 and the 8 slices of the
+    image into slabs of 3, 3 and 2."""
+    outdir, codes, hung = _launch(world, exchange=exchange)
+    errs = [open(os.path.join(outdir, f"err{r}.txt")).read() for r in range(world)
+            if os.path.exists(os.path.join(outdir, f"err{r}.txt"))]
+    assert not hung and codes == [0] * world, errs or codes
     a = np.load(os.path.join(outdir, "img0.npy"))
-    b = np.load(os.path.join(outdir, "img1.npy"))
-    np.testing.assert_array_equal(a, b)
+    for r in range(1, world):
+        np.testing.assert_array_equal(a, np.load(os.path.join(outdir, f"img{r}.npy")))
     w, prm = problem()
     x = workloads.activity(w)
     y = workloads.poisson_counts(restated.forward(w.scanner, w.proj, w.vol, x), w.counts, 4)
@@ -149,12 +168,21 @@ def test_failed_rank_is_reported_not_hung():
 def test_shard_mapping():
     from fir_b200.distributed import Shard
 
-    # rank r's share of subset s of n is subset s + n*r of n*world: views v with
-    # v % (n*world) == s + n*r, which together cover v % n == s exactly once
-    n, world, n_views = 4, 2, 32
-    for s in range(n):
-        views = set()
+    # rank r takes the subset's k-th view for k % world == r: the shares
+    # partition the subset's views v % n == s for any world size, evenly or not
+    n, n_views = 4, 32
+    for world in (1, 2, 3, 5, 8, 9):
+        for s in range(n):
+            shares = [Shard(r, world).views(s, n, n_views) for r in range(world)]
+            flat = sorted(v for sh in shares for v in sh)
+            assert flat == [v for v in range(n_views) if v % n == s]
+            sizes = [len(sh) for sh in shares]
+            assert max(sizes) - min(sizes) <= 1 and sizes == sorted(sizes, reverse=True)
+    # slabs cover the slices once, the last ones possibly short or empty
+    for nz, world in ((8, 3), (64, 8), (5, 8)):
+        covered = []
         for r in range(world):
-            sub, nn = Shard(r, world).subset(s, n)
-            views |= {v for v in range(n_views) if v % nn == sub}
-        assert views == {v for v in range(n_views) if v % n == s}
+            z0, z1, per = Shard(r, world).slab(nz)
+            assert z1 - z0 <= per and per * world >= nz
+            covered += list(range(z0, z1))
+        assert covered == list(range(nz))
