@@ -142,6 +142,9 @@ class Restated:
         L.fo_osem.argtypes = [C.POINTER(FoProj), _f32p, C.c_void_p, C.POINTER(FoVol), C.c_int, _f64p, _f64p,
                               _f32p, _f32p, C.POINTER(FoOsem)]
         L.fo_osem_psf.argtypes = L.fo_osem.argtypes
+        L.fo_precision_study.argtypes = [C.POINTER(FoProj), _f64p, _f64p, C.POINTER(FoVol), C.c_int, _f32p,
+                                         np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS"), C.c_longlong,
+                                         C.c_int, _f64p]
         L.fo_osem_reso_reco.argtypes = [C.POINTER(FoProj), _f32p, C.c_void_p, C.POINTER(FoVol), C.c_int, _f64p,
                                         _f64p, _f32p, _f32p, C.c_int, C.POINTER(FoOsem)]
         L.fo_osem_weighted.argtypes = [C.POINTER(FoProj), _f32p, _f32p, C.c_void_p, C.POINTER(FoVol), C.c_int,
@@ -283,6 +286,18 @@ class Restated:
         self.L.fo_osem_reso_reco(C.byref(f), np.ascontiguousarray(sino, np.float32), bptr, C.byref(fo_vol(v)),
                                  int(truncate), xy, z, img, sens, sens.size // v.n_voxels, C.byref(o))
         return img.reshape(v.shape_zyx), sens
+
+    def precision_study(self, s, p, v, img, bins, precision: int, truncate: bool = True) -> dict:
+        """FIR's double traversal against a float one (precision 1: double
+        set-up, float loop; 2: float set-up and loop) over the given bins."""
+        f = self.proj(p)
+        xy, z = self.scanner_tables(s)
+        out = np.zeros(5, np.float64)
+        b = np.ascontiguousarray(bins, np.int64)
+        self.L.fo_precision_study(C.byref(f), xy, z, C.byref(fo_vol(v)), int(truncate),
+                                  np.ascontiguousarray(img, np.float32).ravel(), b, b.size, int(precision), out)
+        return {"lors": int(out[0]), "lists_differ": int(out[1]), "max_rel_length": float(out[2]),
+                "max_rel_line": float(out[3]), "rms_rel_line": float(out[4])}
 
     def bin_coordinates(self, p: ProjSpec, pairs):
         """[n, 5]: flag, seg, view, axial, tang of each (ring1, crystal1,

@@ -348,6 +348,213 @@ int fo_siddon(const fo_grid* g, double x1, double y1, double z1, double x2, doub
   return 1;
 }
 
+static void lor_ends(const fo_proj* p, const double* xy, const double* z, int seg, int view, int axial, int tang,
+                     double* e);
+
+/* ---- precision study of the traversal (not FIR code) ----
+ * fo_siddon with single-precision arithmetic, to measure how often a float
+ * traversal emits a voxel list different from FIR's double one:
+ *   precision 1: FIR's double set-up (entry/exit alphas, first crossings,
+ *                steps, start voxel), then the loop in float: alphas, their
+ *                running sums, the minimum, the tie test |a - next| < 1e-5
+ *                and the lengths;
+ *   precision 2: the same with the set-up in float as well.
+ * Returns 1 when the segment crosses the volume, like fo_siddon. */
+int fo_siddon_study(const fo_grid* g, const double* e, int precision, int* coords, double* lengths, int cap,
+                    int* count)
+{
+  *count = 0;
+  int pos[3], dir[3];
+  float a[3], da[3], amin_f, amax_f, d12_f;
+  if (precision == 1)
+  {
+    fo_setup s[3];
+    for (int d = 0; d < 3; ++d)
+      if (!dim_setup(g, d, e[d], e[3 + d], &s[d])) return 0;
+    const double amin = dmax(s[0].amin, dmax(s[1].amin, dmax(s[2].amin, 0.0)));
+    const double amax = dmin(s[0].amax, dmin(s[1].amax, dmin(s[2].amax, 1.0)));
+    if (amin >= amax) return 0;
+    const double d12 = sqrt(s[0].diff * s[0].diff + s[1].diff * s[1].diff + s[2].diff * s[2].diff);
+    const int nm1[3] = {g->nx - 1, g->ny - 1, g->nz - 1};
+    for (int d = 0; d < 3; ++d)
+    {
+      const double dad = g->ext[d] / (s[d].diff < 0 ? -s[d].diff : s[d].diff);
+      int ind = (int)((e[d] + s[d].diff * amin - g->low[d]) / g->ext[d]);
+      ind = ind < nm1[d] ? ind : nm1[d];
+      pos[d] = ind > 0 ? ind : 0;
+      double al = s[d].next;
+      if (al < 1.0) al = (g->low[d] + g->ext[d] * pos[d] - e[d]) / s[d].diff;
+      if (s[d].dir > 0) al += dad;
+      a[d] = (float)al;
+      da[d] = (float)dad;
+      dir[d] = s[d].dir;
+    }
+    amin_f = (float)amin;
+    amax_f = (float)amax;
+    d12_f = (float)d12;
+  }
+  else
+  {
+    const float eps = (float)FO_EPS;
+    float diff[3], smin[3], smax[3], snext[3];
+    for (int d = 0; d < 3; ++d)
+    {
+      const float c1 = (float)e[d], c2 = (float)e[3 + d];
+      const float lo = (float)g->low[d], hi = (float)g->high[d];
+      float df = c2 - c1;
+      if ((df < 0 ? -df : df) > eps)
+      {
+        dir[d] = df > 0 ? 1 : -1;
+        smin[d] = df > 0 ? (lo - c1) / df : (hi - c1) / df;
+        smax[d] = df > 0 ? (hi - c1) / df : (lo - c1) / df;
+        snext[d] = 0.0f;
+      }
+      else
+      {
+        if (c1 < lo || c1 > hi) return 0;
+        df = eps;
+        dir[d] = -1;
+        smin[d] = 0.0f;
+        smax[d] = 1.0f;
+        snext[d] = 1.0f;
+      }
+      diff[d] = df;
+    }
+    float t = smin[2] > 0.0f ? smin[2] : 0.0f;
+    t = smin[1] > t ? smin[1] : t;
+    amin_f = smin[0] > t ? smin[0] : t;
+    t = smax[2] < 1.0f ? smax[2] : 1.0f;
+    t = smax[1] < t ? smax[1] : t;
+    amax_f = smax[0] < t ? smax[0] : t;
+    if (amin_f >= amax_f) return 0;
+    d12_f = sqrtf(diff[0] * diff[0] + diff[1] * diff[1] + diff[2] * diff[2]);
+    const int nm1[3] = {g->nx - 1, g->ny - 1, g->nz - 1};
+    for (int d = 0; d < 3; ++d)
+    {
+      const float ext = (float)g->ext[d], lo = (float)g->low[d];
+      da[d] = ext / (diff[d] < 0 ? -diff[d] : diff[d]);
+      int ind = (int)(((float)e[d] + diff[d] * amin_f - lo) / ext);
+      ind = ind < nm1[d] ? ind : nm1[d];
+      pos[d] = ind > 0 ? ind : 0;
+      float al = snext[d];
+      if (al < 1.0f) al = (lo + ext * (float)pos[d] - (float)e[d]) / diff[d];
+      if (dir[d] > 0) al += da[d];
+      a[d] = al;
+    }
+  }
+  const int nm1[3] = {g->nx - 1, g->ny - 1, g->nz - 1};
+  const int row = g->nx, slice = g->nx * g->ny;
+  const float eps = (float)FO_EPS;
+  int n = 0;
+  float prev = amin_f;
+  while (prev < amax_f && n <= cap)
+  {
+    float next = a[0] < a[1] ? a[0] : a[1];
+    next = a[2] < next ? a[2] : next;
+    next = amax_f < next ? amax_f : next;
+    if (pos[0] >= 0 && pos[0] <= nm1[0] && pos[1] >= 0 && pos[1] <= nm1[1] && pos[2] >= 0 && pos[2] <= nm1[2])
+    {
+      if (n < cap)
+      {
+        coords[n] = pos[0] + pos[1] * row + pos[2] * slice;
+        lengths[n] = (double)((next - prev) * d12_f);
+      }
+      ++n;
+    }
+    for (int d = 0; d < 3; ++d)
+    {
+      const float dd = a[d] - next;
+      if ((dd < 0 ? -dd : dd) < eps)
+      {
+        a[d] += da[d];
+        pos[d] += dir[d];
+      }
+    }
+    prev = next;
+  }
+  *count = n;
+  return 1;
+}
+
+/* Precision study over the bins `bins` (n, file-order indices) of sinogram p:
+ * each LOR is traversed by fo_siddon (FIR's double arithmetic) and by
+ * fo_siddon_study(precision).  out[0] LORs crossing the volume, out[1] LORs
+ * whose voxel lists differ (indices or length of the list), out[2] the
+ * largest relative length difference on LORs with equal lists, out[3] the
+ * largest and out[4] the root-mean-square relative difference of the line
+ * integral of img (double sums), over crossing LORs with a non-zero
+ * integral. */
+static void bin_coords(const fo_proj* p, long long bin, int* seg, int* view, int* ax, int* tang)
+{
+  long long b = bin;
+  for (int s = -p->seg_offset; s <= p->seg_offset; ++s)
+  {
+    const int nax = p->n_axial[s + p->seg_offset];
+    const long long n = (long long)nax * p->n_views * p->n_tang_coords;
+    if (b < n)
+    {
+      *seg = s;
+      *view = (int)(b / ((long long)nax * p->n_tang_coords));
+      const long long r = b - (long long)*view * nax * p->n_tang_coords;
+      *ax = (int)(r / p->n_tang_coords);
+      *tang = (int)(r - (long long)*ax * p->n_tang_coords) - p->tang_offset;
+      return;
+    }
+    b -= n;
+  }
+}
+
+void fo_precision_study(const fo_proj* p, const double* xy, const double* z, const fo_vol* v, int truncate,
+                        const float* img, const long long* bins, long long n, int precision, double* out)
+{
+  fo_grid g;
+  fo_grid_init(&g, v, truncate);
+  const int cap = v->nx + v->ny + v->nz + 2;
+  int* c1 = (int*)malloc(sizeof(int) * (size_t)cap * 2);
+  double* l1 = (double*)malloc(sizeof(double) * (size_t)cap * 2);
+  int* c2 = c1 + cap;
+  double* l2 = l1 + cap;
+  double crossing = 0, differ = 0, max_len = 0, max_line = 0, sq_line = 0, n_line = 0;
+  for (long long i = 0; i < n; ++i)
+  {
+    int seg, view, ax, tang;
+    bin_coords(p, bins[i], &seg, &view, &ax, &tang);
+    double e[6];
+    lor_ends(p, xy, z, seg, view, ax, tang, e);
+    int n1 = 0, n2 = 0;
+    const int x1 = fo_siddon(&g, e[0], e[1], e[2], e[3], e[4], e[5], c1, l1, cap, &n1);
+    const int x2 = fo_siddon_study(&g, e, precision, c2, l2, cap, &n2);
+    if (!x1 && !x2) continue;
+    crossing += 1;
+    int same = x1 == x2 && n1 == n2 && n1 <= cap;
+    for (int k = 0; same && k < n1; ++k) same = c1[k] == c2[k];
+    if (!same) differ += 1;
+    else
+      for (int k = 0; k < n1; ++k)
+      {
+        const double d = fabs(l2[k] - l1[k]) / (l1[k] > 0 ? l1[k] : 1.0);
+        if (l1[k] > 1e-9 && d > max_len) max_len = d;
+      }
+    double s1 = 0, s2 = 0;
+    for (int k = 0; k < n1 && k < cap; ++k) s1 += l1[k] * img[c1[k]];
+    for (int k = 0; k < n2 && k < cap; ++k) s2 += l2[k] * img[c2[k]];
+    if (s1 > 0)
+    {
+      const double r = fabs(s2 - s1) / s1;
+      if (r > max_line) max_line = r;
+      sq_line += r * r;
+      n_line += 1;
+    }
+  }
+  out[0] = crossing;
+  out[1] = differ;
+  out[2] = max_len;
+  out[3] = max_line;
+  out[4] = n_line > 0 ? sqrt(sq_line / n_line) : 0.0;
+  free(c1);
+  free(l1);
+}
+
 /* ---- projectors: projections.cc:15-92, :94-184; VolData.cc:357-385 ---- */
 static long long seg_base(const fo_proj* p, int seg)
 {

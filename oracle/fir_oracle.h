@@ -114,6 +114,15 @@ void fo_osem_reso_reco(const fo_proj* p, const float* sino, const float* bias, c
 
 void fo_em_update(long long n, float* img, float* bp, const float* sens);
 
+/* Precision study of the traversal (not FIR code): FIR's double traversal
+ * against a float loop after FIR's double set-up (precision 1) or a float
+ * set-up and loop (precision 2), over n bins of sinogram p.  out[5]: LORs
+ * crossing, LORs with a different voxel list, largest relative length
+ * difference on equal lists, largest and RMS relative difference of the
+ * line integral of img. */
+void fo_precision_study(const fo_proj* p, const double* xy, const double* z, const fo_vol* v, int truncate,
+                        const float* img, const long long* bins, long long n, int precision, double* out);
+
 /* OSEM with per-bin multiplicative factors m (ordinary-Poisson model):
  * estimate m * (A x) + bias; the backprojected value is m * y / estimate. */
 void fo_osem_weighted(const fo_proj* p, const float* sino, const float* mult, const float* bias,
