@@ -385,6 +385,7 @@ def batched_section(args, local):
     t0 = time.perf_counter()
     tune_ms = batch.tune()
     tune_wall = time.perf_counter() - t0
+    tune_table = batch.tune_report()
     shape = batch.launch()
     n_steps, launches = batch.schedule()
     batch.osem(use_graph=True)  # warm: capture + instantiate
@@ -418,6 +419,8 @@ def batched_section(args, local):
         "plain_gpu_launches": plain_launches,
         "launch_shape": {"block": shape[0], "blocks_per_sm": shape[1], "grab": shape[2]},
         "tuner_best_step0_ms": tune_ms,
+        "tuner_candidates": [{"block": b, "blocks_per_sm": p, "grab": gr, "step0_ms": round(t, 4)}
+                             for b, p, gr, t in tune_table],
         "tuner_wall_s": tune_wall,
         "max_rel_l2_vs_plain": err,
         "runs": args.batch_runs,
@@ -434,6 +437,7 @@ def autograd_section(args, local):
     (128x128x48 at 3 mm) with water attenuation and Poisson data; penalized
     Poisson NLL (beta = 0.01, quadratic 26-neighbour); gradient time, adjoint
     test and an L-BFGS reconstruction."""
+    import numpy as np
     import torch
 
     from fir_b200 import autograd as fa
@@ -481,11 +485,33 @@ def autograd_section(args, local):
         if i >= 3:
             times.append(a.elapsed_time(b))
     grad_ms = sum(times) / len(times)
+    # central finite differences (h = 1e-3, float64) of the first phantom's
+    # penalized NLL at 64 random voxels inside the field of view
+    a64, y64 = atten[:1].double(), y[:1].double()
+    xd = (0.5 + 0.5 * torch.rand((1,) + tuple(w0.vol.shape_zyx), generator=g, device=dev,
+                                 dtype=torch.float64)).requires_grad_(True)
+    fa.penalized_nll(xd, y64, op, beta, a64).backward()
+    gd = xd.grad.detach()
+    rng = np.random.default_rng(16)
+    nz, ny, nx = w0.vol.shape_zyx
+    fd_worst, h = 0.0, 1e-3
+    with torch.no_grad():
+        for _ in range(64):
+            while True:
+                j = (0, int(rng.integers(nz)), int(rng.integers(ny)), int(rng.integers(nx)))
+                if (j[2] - ny / 2) ** 2 + (j[3] - nx / 2) ** 2 < 45 ** 2:
+                    break
+            xp, xm = xd.detach().clone(), xd.detach().clone()
+            xp[j] += h
+            xm[j] -= h
+            fd = (float(fa.penalized_nll(xp, y64, op, beta, a64)) - float(fa.penalized_nll(xm, y64, op, beta, a64))) \
+                / (2 * h)
+            fd_worst = max(fd_worst, abs(fd - float(gd[j])) / max(abs(float(gd[j])), 1e-3))
+    del xd, gd, a64, y64
+
     launches0 = op.ctx.launch_count
     xr, stats = fa.reconstruct_lbfgs(op, y, beta, atten, steps=args.lbfgs_steps)
     launches = op.ctx.launch_count - launches0
-    import numpy as np
-
     corr = float(np.corrcoef(xr.cpu().numpy().ravel(), x_true.cpu().numpy().ravel())[0, 1])
     op.close()
     n = len(ws)
@@ -500,6 +526,8 @@ def autograd_section(args, local):
         "frames": n,
         "lors_per_frame": nb,
         "adjoint_rel_error": abs(lhs - rhs) / abs(lhs),
+        "finite_difference_max_rel_error": fd_worst,
+        "finite_difference": "central, h = 1e-3, float64, 64 random voxels of the first phantom inside the FOV",
         "lbfgs_steps": args.lbfgs_steps,
         "lbfgs_evaluations": stats["evaluations"],
         "lbfgs_ms_per_gradient": sum(stats["gradient_ms"]) / max(1, len(stats["gradient_ms"])),

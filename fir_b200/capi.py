@@ -158,6 +158,8 @@ _SIGS = {
     "fir_batch_set_launch": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "fir_batch_get_launch": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "fir_batch_tune": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "fir_batch_tune_report": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.POINTER(C.c_int)]),
     "fir_batch_schedule": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
     "fir_batch_osem": (C.c_int, [C.c_void_p, C.c_int]),
 }
@@ -634,6 +636,17 @@ class Batch:
         ms = C.c_double()
         _check(lib().fir_batch_tune(self._h, C.byref(ms)))
         return ms.value
+
+    def tune_report(self):
+        """The last tune's candidates: [(block, blocks_per_sm, grab, ms), ...]."""
+        n = C.c_int()
+        _check(lib().fir_batch_tune_report(self._h, 0, None, None, None, None, C.byref(n)))
+        k = n.value
+        blk, per, grab = (np.zeros(max(k, 1), np.int32) for _ in range(3))
+        ms = np.zeros(max(k, 1), np.float64)
+        _check(lib().fir_batch_tune_report(self._h, k, blk.ctypes.data, per.ctypes.data, grab.ctypes.data,
+                                           ms.ctypes.data, C.byref(n)))
+        return [(int(blk[i]), int(per[i]), int(grab[i]), float(ms[i])) for i in range(k)]
 
     def schedule(self):
         """(steps, kernel launches) of the whole schedule."""

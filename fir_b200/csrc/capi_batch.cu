@@ -59,6 +59,8 @@ struct fir_batch
   Launch all;
   std::vector<Step> steps;
   BatchLaunch shape{128, 0, 1};
+  // the last fir_batch_tune: every candidate shape with its best time (ms)
+  std::vector<std::pair<BatchLaunch, double>> tuned;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   long long schedule_launches = 0;
@@ -570,6 +572,7 @@ fir_status fir_batch_tune(fir_batch* batch, double* best_ms)
     cuda_ok(cudaEventCreate(&e1), "cudaEventCreate");
     double best = 1e300;
     BatchLaunch pick = b.shape;
+    b.tuned.clear();
     try
     {
       batch_begin(b);
@@ -592,6 +595,7 @@ fir_status fir_batch_tune(fir_batch* batch, double* best_ms)
           cuda_ok(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
           t_min = std::min(t_min, (double)ms);
         }
+        b.tuned.emplace_back(L, t_min);
         if (t_min < best)
         {
           best = t_min;
@@ -619,6 +623,34 @@ fir_status fir_batch_tune(fir_batch* batch, double* best_ms)
       *best_ms = best;
     }
     read_checks(*b.ctx);
+  });
+}
+
+fir_status fir_batch_tune_report(const fir_batch* batch, int max, int* block, int* blocks_per_sm, int* grab,
+                                 double* ms, int* n)
+{
+  return guarded(__func__, [&] {
+    if (batch == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "batch is NULL");
+    }
+    const int count = (int)batch->tuned.size();
+    if (n != nullptr)
+    {
+      *n = count;
+    }
+    for (int i = 0; i < count && i < max; ++i)
+    {
+      const auto& t = batch->tuned[(size_t)i];
+      if (block != nullptr)
+        block[i] = t.first.block;
+      if (blocks_per_sm != nullptr)
+        blocks_per_sm[i] = t.first.blocks_per_sm;
+      if (grab != nullptr)
+        grab[i] = t.first.grab;
+      if (ms != nullptr)
+        ms[i] = t.second;
+    }
   });
 }
 

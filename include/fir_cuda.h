@@ -419,6 +419,12 @@ fir_status fir_batch_get_launch(const fir_batch* batch, int* block, int* blocks_
  * each candidate launch shape and keeps the fastest; *best_ms (may be NULL)
  * receives its time.  It uses the current images without changing them. */
 fir_status fir_batch_tune(fir_batch* batch, double* best_ms);
+/* The candidates of the last fir_batch_tune with their times: *n receives
+ * their number; the first `max` are written to the arrays (each may be
+ * NULL): block, blocks_per_sm, grab as fir_batch_set_launch takes them, and
+ * the best of two timed runs of step 0's projector in ms. */
+fir_status fir_batch_tune_report(const fir_batch* batch, int max, int* block, int* blocks_per_sm, int* grab,
+                                 double* ms, int* n);
 /* Number of steps (the largest number of sub-iterations of any problem) and
  * number of kernel launches of the whole schedule. */
 fir_status fir_batch_schedule(const fir_batch* batch, int* n_steps, long long* n_launches);

@@ -11,6 +11,10 @@ projectors under it (fir_forward_frames / fir_backward_frames).
 * the NLL gradient equals FIR's own BackProj of the ratio sinogram
   a * (1 - y / ybar) to 1e-5 relative L2;
 * L-BFGS lowers the penalized NLL.
+
+The finite-difference and FIR-BackProj checks run on the small workload and
+again at the differentiable-projector workload's scale (clinical scanner,
+3.28e7 LORs, one 128x128x48 phantom).
 """
 import numpy as np
 import pytest
@@ -135,3 +139,65 @@ def test_lbfgs_lowers_the_objective(small):
     assert torch.isfinite(x).all() and float(x.min()) >= 0.0
     c = np.corrcoef(x.cpu().numpy().ravel(), x_true.cpu().numpy().ravel())[0, 1]
     assert c > 0.3, c  # 10 steps from a uniform start: partly converged
+
+
+# ---- the same checks at the differentiable-projector workload's scale: the
+# clinical scanner (32 rings x 512 crystals, 125 tangential bins, 3.28e7
+# LORs) and one 128x128x48 phantom at 3 mm with water attenuation
+
+@pytest.fixture(scope="module")
+def clinical_frame():
+    w = workloads.autograd_batch(1)[0]
+    op = fa.SiddonProjector(w.scanner, w.proj, w.vol)
+    yield w, op
+    op.close()
+
+
+def test_gradient_matches_finite_differences_at_scale(clinical_frame):
+    """Central differences, h = 1e-3, on 64 random voxels of the field of
+    view, float64: 1e-3 relative."""
+    w, op = clinical_frame
+    atten, y, x_true = _data(w, op, torch.float64)
+    x = (0.5 + 0.5 * rand_images(w, 1, 15, torch.float64)[0]).requires_grad_(True)
+    beta = 0.01
+    loss = fa.penalized_nll(x, y, op, beta, atten)
+    loss.backward()
+    grad = x.grad.detach()
+    rng = np.random.default_rng(16)
+    nz, ny, nx = w.vol.shape_zyx
+    h = 1e-3
+    worst = 0.0
+    with torch.no_grad():
+        for _ in range(64):
+            # within 45 voxels (135 mm) of the axis, inside the 150 mm field of view
+            while True:
+                j = (int(rng.integers(nz)), int(rng.integers(ny)), int(rng.integers(nx)))
+                if (j[1] - ny / 2) ** 2 + (j[2] - nx / 2) ** 2 < 45 ** 2:
+                    break
+            xp = x.detach().clone()
+            xp[j] += h
+            xm = x.detach().clone()
+            xm[j] -= h
+            fd = (float(fa.penalized_nll(xp, y, op, beta, atten)) - float(fa.penalized_nll(xm, y, op, beta, atten))) \
+                / (2 * h)
+            g = float(grad[j])
+            worst = max(worst, abs(fd - g) / max(abs(g), 1e-3))
+    assert worst <= 1e-3, worst
+
+
+def test_nll_gradient_equals_fir_backprojection_at_scale(clinical_frame, reference):
+    """The NLL gradient of the float32 path against FIR's own BackProj of the
+    ratio sinogram (oracle/_ref, all host threads): 1e-5 relative L2."""
+    import os
+
+    w, op = clinical_frame
+    atten, y, _ = _data(w, op, torch.float32)
+    x = (0.5 + rand_images(w, 1, 17)[0]).requires_grad_(True)
+    ybar = fa.expected_counts(x, op, atten)
+    fa.poisson_nll(ybar, y).backward()
+    with torch.no_grad():
+        ratio = ((1.0 - y / ybar) * atten).cpu().numpy()
+    reference.threads(os.cpu_count() or 1)
+    want = reference.backward(w.scanner, w.proj, w.vol, ratio, 1).reshape(w.vol.shape_zyx)
+    got = x.grad.cpu().numpy()
+    assert np.linalg.norm(got - want) <= 1e-5 * np.linalg.norm(want)
