@@ -417,10 +417,11 @@ def batched_section(args, local):
         "schedule_steps": n_steps,
         "gpu_launches": launches,
         "plain_gpu_launches": plain_launches,
-        "launch_shape": {"block": shape[0], "blocks_per_sm": shape[1], "grab": shape[2]},
+        "launch_shape": {"block": shape[0], "blocks_per_sm": shape[1], "grab": shape[2],
+                         "axial_tile": batch.bundle()},
         "tuner_best_step0_ms": tune_ms,
-        "tuner_candidates": [{"block": b, "blocks_per_sm": p, "grab": gr, "step0_ms": round(t, 4)}
-                             for b, p, gr, t in tune_table],
+        "tuner_candidates": [{"block": b, "blocks_per_sm": p, "grab": gr, "axial_tile": at, "step0_ms": round(t, 4)}
+                             for b, p, gr, at, t in tune_table],
         "tuner_wall_s": tune_wall,
         "max_rel_l2_vs_plain": err,
         "runs": args.batch_runs,

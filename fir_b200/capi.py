@@ -159,7 +159,9 @@ _SIGS = {
     "fir_batch_get_launch": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "fir_batch_tune": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "fir_batch_tune_report": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                        C.POINTER(C.c_int)]),
+                                        C.c_void_p, C.POINTER(C.c_int)]),
+    "fir_batch_set_bundle": (C.c_int, [C.c_void_p, C.c_int]),
+    "fir_batch_get_bundle": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "fir_batch_schedule": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
     "fir_batch_osem": (C.c_int, [C.c_void_p, C.c_int]),
 }
@@ -638,15 +640,25 @@ class Batch:
         return ms.value
 
     def tune_report(self):
-        """The last tune's candidates: [(block, blocks_per_sm, grab, ms), ...]."""
+        """The last tune's candidates: [(block, blocks_per_sm, grab, axial_tile, ms), ...]."""
         n = C.c_int()
-        _check(lib().fir_batch_tune_report(self._h, 0, None, None, None, None, C.byref(n)))
+        _check(lib().fir_batch_tune_report(self._h, 0, None, None, None, None, None, C.byref(n)))
         k = n.value
-        blk, per, grab = (np.zeros(max(k, 1), np.int32) for _ in range(3))
+        blk, per, grab, tile = (np.zeros(max(k, 1), np.int32) for _ in range(4))
         ms = np.zeros(max(k, 1), np.float64)
         _check(lib().fir_batch_tune_report(self._h, k, blk.ctypes.data, per.ctypes.data, grab.ctypes.data,
-                                           ms.ctypes.data, C.byref(n)))
-        return [(int(blk[i]), int(per[i]), int(grab[i]), float(ms[i])) for i in range(k)]
+                                           tile.ctypes.data, ms.ctypes.data, C.byref(n)))
+        return [(int(blk[i]), int(per[i]), int(grab[i]), int(tile[i]), float(ms[i])) for i in range(k)]
+
+    def set_bundle(self, axial_tile: int) -> None:
+        """Bundle shape: 0, 32 consecutive LORs; A in (1, 2, 4, 8), A axial
+        planes x 32 / A tangential bins."""
+        _check(lib().fir_batch_set_bundle(self._h, int(axial_tile)))
+
+    def bundle(self) -> int:
+        a = C.c_int()
+        _check(lib().fir_batch_get_bundle(self._h, C.byref(a)))
+        return a.value
 
     def schedule(self):
         """(steps, kernel launches) of the whole schedule."""

@@ -48,13 +48,46 @@ __device__ __forceinline__ int take(int* queue, int grab, int lane)
   return __shfl_sync(0xffffffffu, v, 0);
 }
 
+// Enumerated index of lane `lane` of bundle j of a tiled launch shape: tile
+// (ta, tt) of A axial planes x 32 / A tangential bins in the (segment, view)
+// plane of the subset's enumeration; lanes past the plane's edges get
+// n_enum (idle).
+__device__ __forceinline__ int tiled_lor(const Sino& s, const int* __restrict__ base, int j, int A, int lane)
+{
+  int lo = 0, hi = s.n_segments;
+  while (hi - lo > 1)
+  {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(base + mid) <= j)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const int T = 32 / A;
+  const int nax = s.n_axial[lo];
+  const int tiles_t = (s.n_tang + T - 1) / T;
+  const int per_view = ((nax + A - 1) / A) * tiles_t;
+  const int r = j - __ldg(base + lo);
+  const int sv = r / per_view;
+  const int rem = r - sv * per_view;
+  const int ta = rem / tiles_t;
+  const int a = ta * A + lane / T;
+  const int t = (rem - ta * tiles_t) * T + lane % T;
+  if (a >= nax || t >= s.n_tang)
+  {
+    return s.n_enum;
+  }
+  return s.enum_base[lo] + (sv * nax + a) * s.n_tang + t;
+}
+
 // TImg: what the projection gathers from, each problem's double copy or (for
 // problems whose double copy does not fit in L2 beside the accumulator) its
 // float image.  A launch covers problems of one kind.
 template<bool kPersistent, typename TImg>
 __global__ void __launch_bounds__(256, 4) k_batch_osem(const BatchProblem* __restrict__ P,
                                                     const BatchItem* __restrict__ items, int n_items,
-                                                    int n_bundles, int* queue, int grab, int* check)
+                                                    int n_bundles, int* queue, int grab, int axial_tile,
+                                                    int* check)
 {
   const int lane = threadIdx.x & 31;
   int b = kPersistent ? take(queue, grab, lane) : (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -68,7 +101,8 @@ __global__ void __launch_bounds__(256, 4) k_batch_osem(const BatchProblem* __res
       const int p = __ldg(&items[it].problem);
       const int subset = __ldg(&items[it].subset);
       const BatchProblem& pb = P[p];
-      const int i = (k - __ldg(&items[it].unit_begin)) * 32 + lane;
+      const int j = k - __ldg(&items[it].unit_begin);
+      const int i = axial_tile == 0 ? j * 32 + lane : tiled_lor(pb.s, pb.bundle_base, j, axial_tile, lane);
       if constexpr (sizeof(TImg) == sizeof(double))
       {
         osem_lor(pb.g, pb.s, subset, pb.t, pb.wide, pb.wide_t, pb.sino, pb.bias, pb.bp, pb.bp_t, pb.skip_zero != 0,
@@ -299,7 +333,7 @@ void project(const BatchProblem* P, const BatchItem* items, int n_items, int n_b
   if (L.blocks_per_sm <= 0)
   {
     k_batch_osem<false, TImg><<<(unsigned)plain_blocks, L.block, 0, stream>>>(P, items, n_items, n_bundles,
-                                                                               nullptr, 1, check);
+                                                                               nullptr, 1, L.axial_tile, check);
     return;
   }
   long long blocks = (long long)n_sms * L.blocks_per_sm;
@@ -308,7 +342,7 @@ void project(const BatchProblem* P, const BatchItem* items, int n_items, int n_b
     blocks = plain_blocks;
   }
   k_batch_osem<true, TImg><<<(unsigned)blocks, L.block, 0, stream>>>(P, items, n_items, n_bundles, queue, L.grab,
-                                                                      check);
+                                                                      L.axial_tile, check);
 }
 }  // namespace
 
@@ -357,6 +391,36 @@ void launch_batch_filter(const BatchProblem* P, const BatchItem* items, int n_it
   {
     k_batch_filter<2><<<n_units, kBatchBlock, 0, stream>>>(P, items, n_items);
   }
+}
+
+long long batch_bundles(const Sino& s, int axial_tile)
+{
+  if (axial_tile == 0)
+  {
+    return ((long long)s.n_enum + 31) / 32;
+  }
+  long long n = 0;
+  const int T = 32 / axial_tile;
+  const int vps = s.n_views / s.n_subsets;
+  for (int k = 0; k < s.n_segments; ++k)
+  {
+    n += (long long)vps * ((s.n_axial[k] + axial_tile - 1) / axial_tile) * ((s.n_tang + T - 1) / T);
+  }
+  return n;
+}
+
+void batch_bundle_bases(const Sino& s, int axial_tile, int* base)
+{
+  long long n = 0;
+  const int A = axial_tile > 0 ? axial_tile : 1;
+  const int T = 32 / A;
+  const int vps = s.n_views / s.n_subsets;
+  for (int k = 0; k < s.n_segments; ++k)
+  {
+    base[k] = (int)n;
+    n += (long long)vps * ((s.n_axial[k] + A - 1) / A) * ((s.n_tang + T - 1) / T);
+  }
+  base[s.n_segments] = (int)n;
 }
 
 int batch_max_resident(int block)

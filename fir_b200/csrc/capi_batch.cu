@@ -208,6 +208,99 @@ void batch_copy(fir_batch& b, void* dst, const void* src, size_t bytes)
   cuda_ok(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, b.ctx->stream), "cudaMemcpyAsync");
 }
 
+// Builds the item lists of the whole schedule for the current launch shape
+// (its bundle form sets the projector's work units) and uploads them with the
+// problem descriptors; waits for the copies.
+void build_schedule(fir_batch& b)
+{
+  const int n_problems = b.n;
+  for (int k = 0; k < n_problems; ++k)
+  {
+    batch_bundle_bases(b.desc_host[(size_t)k].s, b.shape.axial_tile, b.desc_host[(size_t)k].bundle_base);
+  }
+  b.steps.clear();
+  std::vector<BatchItem> items;
+  std::vector<int> all((size_t)n_problems), zeros((size_t)n_problems, 0);
+  for (int k = 0; k < n_problems; ++k)
+  {
+    all[(size_t)k] = k;
+  }
+  auto vox_units = [&](int k) { return (b.pr[(size_t)k].v.nvox + kBatchBlock - 1) / kBatchBlock; };
+  auto lor_units = [&](int k) { return batch_bundles(b.desc_host[(size_t)k].s, b.shape.axial_tile); };
+  b.all = add_launch(items, all, zeros, zeros, vox_units);
+  std::vector<int> order = all;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return b.pr[(size_t)x].path > b.pr[(size_t)y].path; });
+  int n_steps = 0;
+  for (const auto& q : b.pr)
+  {
+    n_steps = std::max(n_steps, q.n_sub_total);
+  }
+  for (int t = 0; t < n_steps; ++t)
+  {
+    std::vector<int> probs, subs, filts, fprobs, fsubs, fflags, dprobs, dsubs, dfilts, gprobs, gsubs, gfilts;
+    for (int k : order)
+    {
+      const fir_batch::Problem& q = b.pr[(size_t)k];
+      if (t >= q.n_sub_total)
+      {
+        continue;
+      }
+      const int subiter = t + 1;
+      const int f = q.filter && subiter % q.prm.convolution_interval == 0 ? 1 : 0;
+      probs.push_back(k);
+      subs.push_back(t % q.n_subsets);
+      filts.push_back(f);
+      (q.gather_float ? gprobs : dprobs).push_back(k);
+      (q.gather_float ? gsubs : dsubs).push_back(t % q.n_subsets);
+      (q.gather_float ? gfilts : dfilts).push_back(f);
+      if (f)
+      {
+        fprobs.push_back(k);
+        fsubs.push_back(t % q.n_subsets);
+        fflags.push_back(1);
+      }
+    }
+    fir_batch::Step st;
+    st.proj = add_launch(items, dprobs, dsubs, dfilts, lor_units);
+    st.proj_f = add_launch(items, gprobs, gsubs, gfilts, lor_units);
+    st.em = add_launch(items, probs, subs, filts, vox_units);
+    st.filt = add_launch(items, fprobs, fsubs, fflags, vox_units);
+    b.steps.push_back(st);
+  }
+  b.desc.ensure(b.desc_host.size() * sizeof(BatchProblem));
+  batch_copy(b, b.desc.p, b.desc_host.data(), b.desc_host.size() * sizeof(BatchProblem));
+  b.items.ensure(std::max<size_t>(items.size(), 1) * sizeof(BatchItem));
+  batch_copy(b, b.items.p, items.data(), items.size() * sizeof(BatchItem));
+  b.queue.ensure(std::max<size_t>(2 * b.steps.size(), 1) * sizeof(int));
+  cuda_ok(cudaStreamSynchronize(b.ctx->stream), "cudaStreamSynchronize");
+  b.schedule_launches = 1;
+  for (const auto& st : b.steps)
+  {
+    b.schedule_launches += 1 + (st.proj.n_items > 0 ? 1 : 0) + (st.proj_f.n_items > 0 ? 1 : 0) +
+                           (st.filt.n_items > 0 ? 3 : 0);
+  }
+}
+
+// Makes s the launch shape: drops the captured graph, and rebuilds the
+// schedule when the bundle form changes.
+void set_shape(fir_batch& b, const BatchLaunch& s)
+{
+  const BatchLaunch& o = b.shape;
+  if (s.block == o.block && s.blocks_per_sm == o.blocks_per_sm && s.grab == o.grab && s.axial_tile == o.axial_tile)
+  {
+    return;
+  }
+  cuda_ok(cudaStreamSynchronize(b.stream), "cudaStreamSynchronize");
+  drop_graph(b);
+  const bool rebuild = s.axial_tile != o.axial_tile;
+  b.shape = s;
+  if (rebuild)
+  {
+    build_schedule(b);
+  }
+}
+
 // Orders the batch's stream after the context's stream.
 void batch_begin(fir_batch& b)
 {
@@ -338,68 +431,7 @@ fir_status fir_batch_create(fir_batch** out, fir_ctx* ctx, int n_problems, const
           d.tz = gauss_taps(q.prm.fwhm_xyz[2], q.v.d.voxel_z, true);
         }
       }
-      // item lists
-      std::vector<BatchItem> items;
-      std::vector<int> all((size_t)n_problems), zeros((size_t)n_problems, 0);
-      for (int k = 0; k < n_problems; ++k)
-      {
-        all[(size_t)k] = k;
-      }
-      auto vox_units = [&](int k) { return (b->pr[(size_t)k].v.nvox + kBatchBlock - 1) / kBatchBlock; };
-      auto lor_units = [&](int k) { return ((long long)b->pr[(size_t)k].n_enum + 31) / 32; };
-      b->all = add_launch(items, all, zeros, zeros, vox_units);
-      std::vector<int> order = all;
-      std::stable_sort(order.begin(), order.end(),
-                       [&](int x, int y) { return b->pr[(size_t)x].path > b->pr[(size_t)y].path; });
-      int n_steps = 0;
-      for (const auto& q : b->pr)
-      {
-        n_steps = std::max(n_steps, q.n_sub_total);
-      }
-      for (int t = 0; t < n_steps; ++t)
-      {
-        std::vector<int> probs, subs, filts, fprobs, fsubs, fflags, dprobs, dsubs, dfilts, gprobs, gsubs, gfilts;
-        for (int k : order)
-        {
-          const fir_batch::Problem& q = b->pr[(size_t)k];
-          if (t >= q.n_sub_total)
-          {
-            continue;
-          }
-          const int subiter = t + 1;
-          const int f = q.filter && subiter % q.prm.convolution_interval == 0 ? 1 : 0;
-          probs.push_back(k);
-          subs.push_back(t % q.n_subsets);
-          filts.push_back(f);
-          (q.gather_float ? gprobs : dprobs).push_back(k);
-          (q.gather_float ? gsubs : dsubs).push_back(t % q.n_subsets);
-          (q.gather_float ? gfilts : dfilts).push_back(f);
-          if (f)
-          {
-            fprobs.push_back(k);
-            fsubs.push_back(t % q.n_subsets);
-            fflags.push_back(1);
-          }
-        }
-        fir_batch::Step st;
-        st.proj = add_launch(items, dprobs, dsubs, dfilts, lor_units);
-        st.proj_f = add_launch(items, gprobs, gsubs, gfilts, lor_units);
-        st.em = add_launch(items, probs, subs, filts, vox_units);
-        st.filt = add_launch(items, fprobs, fsubs, fflags, vox_units);
-        b->steps.push_back(st);
-      }
-      b->desc.ensure(b->desc_host.size() * sizeof(BatchProblem));
-      batch_copy(*b, b->desc.p, b->desc_host.data(), b->desc_host.size() * sizeof(BatchProblem));
-      b->items.ensure(std::max<size_t>(items.size(), 1) * sizeof(BatchItem));
-      batch_copy(*b, b->items.p, items.data(), items.size() * sizeof(BatchItem));
-      b->queue.ensure(std::max<size_t>(2 * b->steps.size(), 1) * sizeof(int));
-      cuda_ok(cudaStreamSynchronize(c.stream), "cudaStreamSynchronize");
-      b->schedule_launches = 1;
-      for (const auto& st : b->steps)
-      {
-        b->schedule_launches += 1 + (st.proj.n_items > 0 ? 1 : 0) + (st.proj_f.n_items > 0 ? 1 : 0) +
-                                (st.filt.n_items > 0 ? 3 : 0);
-      }
+      build_schedule(*b);
     }
     catch (...)
     {
@@ -501,13 +533,34 @@ fir_status fir_batch_set_launch(fir_batch* batch, int block, int blocks_per_sm, 
       fail(FIR_ERR_INVALID_ARGUMENT, "blocks per SM must be >= 0 and grab in [1, 64]");
     }
     const int fit = batch_max_resident(block);
-    const BatchLaunch s{block, blocks_per_sm > fit ? fit : blocks_per_sm, grab};
-    if (s.block != b.shape.block || s.blocks_per_sm != b.shape.blocks_per_sm || s.grab != b.shape.grab)
+    const BatchLaunch s{block, blocks_per_sm > fit ? fit : blocks_per_sm, grab, b.shape.axial_tile};
+    set_shape(b, s);
+  });
+}
+
+fir_status fir_batch_set_bundle(fir_batch* batch, int axial_tile)
+{
+  return guarded(__func__, [&] {
+    fir_batch& b = check_batch(batch);
+    if (axial_tile != 0 && axial_tile != 1 && axial_tile != 2 && axial_tile != 4 && axial_tile != 8)
     {
-      cuda_ok(cudaStreamSynchronize(b.stream), "cudaStreamSynchronize");
-      drop_graph(b);
-      b.shape = s;
+      fail(FIR_ERR_INVALID_ARGUMENT, "axial tile must be 0, 1, 2, 4 or 8");
     }
+    BatchLaunch s = b.shape;
+    s.axial_tile = axial_tile;
+    set_shape(b, s);
+  });
+}
+
+fir_status fir_batch_get_bundle(const fir_batch* batch, int* axial_tile)
+{
+  return guarded(__func__, [&] {
+    if (batch == nullptr)
+    {
+      fail(FIR_ERR_INVALID_ARGUMENT, "batch is NULL");
+    }
+    if (axial_tile != nullptr)
+      *axial_tile = batch->shape.axial_tile;
   });
 }
 
@@ -551,19 +604,28 @@ fir_status fir_batch_tune(fir_batch* batch, double* best_ms)
         *best_ms = 0.0;
       return;
     }
-    const auto* P = static_cast<const BatchProblem*>(b.desc.p);
-    const auto* I = static_cast<const BatchItem*>(b.items.p);
+    const BatchProblem* P = static_cast<const BatchProblem*>(b.desc.p);
+    const BatchItem* I = static_cast<const BatchItem*>(b.items.p);
     int* queue = static_cast<int*>(b.queue.p);
+    // linear bundles: every residency and grab; tiled bundles (A axial
+    // planes x 32 / A tangential bins): one warp per bundle or a persistent
+    // grid at full residency
     std::vector<BatchLaunch> cand;
-    for (int block : {64, 128, 256})
+    for (int tile : {0, 1, 2, 4})
     {
-      cand.push_back(BatchLaunch{block, 0, 1});
-      const int fit = batch_max_resident(block);
-      for (int per_sm : {fit, std::max(1, fit / 2)})
+      for (int block : {64, 128, 256})
       {
-        for (int grab : {1, 2, 4})
+        cand.push_back(BatchLaunch{block, 0, 1, tile});
+        const int fit = batch_max_resident(block);
+        for (int per_sm : {fit, std::max(1, fit / 2)})
         {
-          cand.push_back(BatchLaunch{block, per_sm, grab});
+          for (int grab : {1, 2, 4})
+          {
+            if (tile == 0 || (per_sm == fit && grab == 1))
+            {
+              cand.push_back(BatchLaunch{block, per_sm, grab, tile});
+            }
+          }
         }
       }
     }
@@ -572,12 +634,23 @@ fir_status fir_batch_tune(fir_batch* batch, double* best_ms)
     cuda_ok(cudaEventCreate(&e1), "cudaEventCreate");
     double best = 1e300;
     BatchLaunch pick = b.shape;
+    const BatchLaunch start = b.shape;
     b.tuned.clear();
     try
     {
       batch_begin(b);
       for (const BatchLaunch& L : cand)
       {
+        if (L.axial_tile != b.shape.axial_tile)
+        {
+          // the bundle form sets the projector's work units
+          BatchLaunch s = b.shape;
+          s.axial_tile = L.axial_tile;
+          set_shape(b, s);
+          P = static_cast<const BatchProblem*>(b.desc.p);
+          I = static_cast<const BatchItem*>(b.items.p);
+          queue = static_cast<int*>(b.queue.p);
+        }
         double t_min = 1e300;
         for (int rep = 0; rep < 2; ++rep)
         {
@@ -608,16 +681,13 @@ fir_status fir_batch_tune(fir_batch* batch, double* best_ms)
     {
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
+      set_shape(b, start);
       throw;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     b.ctx->launches += (long long)cand.size() * 4;
-    if (pick.block != b.shape.block || pick.blocks_per_sm != b.shape.blocks_per_sm || pick.grab != b.shape.grab)
-    {
-      drop_graph(b);
-      b.shape = pick;
-    }
+    set_shape(b, pick);
     if (best_ms != nullptr)
     {
       *best_ms = best;
@@ -627,7 +697,7 @@ fir_status fir_batch_tune(fir_batch* batch, double* best_ms)
 }
 
 fir_status fir_batch_tune_report(const fir_batch* batch, int max, int* block, int* blocks_per_sm, int* grab,
-                                 double* ms, int* n)
+                                 int* axial_tile, double* ms, int* n)
 {
   return guarded(__func__, [&] {
     if (batch == nullptr)
@@ -648,6 +718,8 @@ fir_status fir_batch_tune_report(const fir_batch* batch, int max, int* block, in
         blocks_per_sm[i] = t.first.blocks_per_sm;
       if (grab != nullptr)
         grab[i] = t.first.grab;
+      if (axial_tile != nullptr)
+        axial_tile[i] = t.first.axial_tile;
       if (ms != nullptr)
         ms[i] = t.second;
     }

@@ -144,6 +144,9 @@ struct BatchProblem
   float cut;   // cut radius (0: none)
   float fwhm;  // max(fwhm x, fwhm y), for the filter's edge restore
   Taps tx, ty, tz;
+  // bundles of the launch shape's tiled form (axial_tile > 0): first bundle
+  // of each segment of one subset's enumeration
+  int bundle_base[kMaxSegments + 1];
 };
 
 // One problem's share of one batched launch.  Work units are numbered
@@ -164,7 +167,15 @@ struct BatchLaunch
   int block;          // threads per block of the projector
   int blocks_per_sm;  // 0: a warp per bundle, no persistence
   int grab;           // bundles taken per queue access by a persistent warp
+  // shape of a bundle (the 32 LORs of a warp): 0, 32 consecutive enumerated
+  // LORs; A = 1, 2, 4 or 8, a tile of A axial planes x 32 / A tangential
+  // bins of one (segment, view), padded at the plane's edges
+  int axial_tile;
 };
+
+// Bundles of one subset of a problem with the given axial tile (0: linear).
+long long batch_bundles(const Sino& s, int axial_tile);
+void batch_bundle_bases(const Sino& s, int axial_tile, int* base);
 
 // wide = cut(img), bp = 0 (and img = cut(img) when write_img).
 void launch_batch_prepare(const BatchProblem* P, const BatchItem* items, int n_items, int n_units,

@@ -415,16 +415,26 @@ fir_status fir_batch_get_image(fir_batch* batch, int p, float* img);
  * capped at what fits), and bundles taken per queue access (1..64). */
 fir_status fir_batch_set_launch(fir_batch* batch, int block, int blocks_per_sm, int grab);
 fir_status fir_batch_get_launch(const fir_batch* batch, int* block, int* blocks_per_sm, int* grab);
+/* Shape of the projector's LOR bundles (the 32 LORs one warp traces
+ * together): 0 (default), 32 consecutive LORs of the enumeration, i.e.
+ * neighbouring tangential bins; A = 1, 2, 4 or 8, tiles of A neighbouring
+ * axial planes x 32 / A neighbouring tangential bins of one (segment, view),
+ * padded with idle lanes at the planes' edges.  The result is the same for
+ * every shape up to the order of the float atomic additions. */
+fir_status fir_batch_set_bundle(fir_batch* batch, int axial_tile);
+fir_status fir_batch_get_bundle(const fir_batch* batch, int* axial_tile);
 /* Autotuner: times the projector of step 0 (all problems' first subsets) for
- * each candidate launch shape and keeps the fastest; *best_ms (may be NULL)
- * receives its time.  It uses the current images without changing them. */
+ * each candidate launch shape (bundle shape, block size, residency, grab)
+ * and keeps the fastest; *best_ms (may be NULL) receives its time.  It uses
+ * the current images without changing them. */
 fir_status fir_batch_tune(fir_batch* batch, double* best_ms);
 /* The candidates of the last fir_batch_tune with their times: *n receives
  * their number; the first `max` are written to the arrays (each may be
- * NULL): block, blocks_per_sm, grab as fir_batch_set_launch takes them, and
- * the best of two timed runs of step 0's projector in ms. */
+ * NULL): block, blocks_per_sm, grab as fir_batch_set_launch takes them,
+ * axial_tile as fir_batch_set_bundle takes it, and the best of two timed
+ * runs of step 0's projector in ms. */
 fir_status fir_batch_tune_report(const fir_batch* batch, int max, int* block, int* blocks_per_sm, int* grab,
-                                 double* ms, int* n);
+                                 int* axial_tile, double* ms, int* n);
 /* Number of steps (the largest number of sub-iterations of any problem) and
  * number of kernel launches of the whole schedule. */
 fir_status fir_batch_schedule(const fir_batch* batch, int* n_steps, long long* n_launches);

@@ -6,7 +6,8 @@ backprojection, so the images agree to 1e-5 relative L2.  Against the oracle
 the bar is the 1e-4 relative L2 of OSEM parity.
 
 The CUDA graph replay, the direct launches and every launch shape (plain or
-persistent, any grab) must give the same images within the same tolerance.
+persistent, any grab, linear or tiled LOR bundles) must give the same images
+within the same tolerance.
 """
 import numpy as np
 import pytest
@@ -119,6 +120,30 @@ def test_launch_shapes_agree(shape):
     ctx.close()
 
 
+@pytest.mark.parametrize("tile,shape", [(1, (128, 0, 1)), (2, (64, 0, 1)), (4, (128, 64, 1)), (8, (256, 2, 2))])
+def test_bundle_shapes_agree(tile, shape):
+    """Tiled bundles (tile axial planes x 32 / tile tangential bins, padded
+    at the planes' edges) cover every LOR once: same images as fir_osem."""
+    ws = mixed_problems()
+    ctx, batch, data = build(ws)
+    want = plain(ws, data)
+    batch.set_launch(*shape)
+    batch.set_bundle(tile)
+    assert batch.bundle() == tile
+    reset(batch, ws)
+    batch.osem(use_graph=True)
+    for k in range(len(ws)):
+        assert rel(batch.get_image(k), want[k]) <= TOL_ATOMIC, (tile, k)
+    # back to linear bundles: the schedule is rebuilt
+    batch.set_bundle(0)
+    reset(batch, ws)
+    batch.osem(use_graph=False)
+    for k in range(len(ws)):
+        assert rel(batch.get_image(k), want[k]) <= TOL_ATOMIC
+    batch.close()
+    ctx.close()
+
+
 def test_tuner_keeps_images_and_results(restated):
     ws = mixed_problems()[:2]
     ctx, batch, data = build(ws, bias_for=())
@@ -127,6 +152,10 @@ def test_tuner_keeps_images_and_results(restated):
     assert ms > 0
     blk, per_sm, grab = batch.launch()
     assert blk in (64, 128, 256) and grab in (1, 2, 4)
+    assert batch.bundle() in (0, 1, 2, 4)
+    table = batch.tune_report()
+    assert len(table) == 3 * 7 + 3 * 3 * 2 and min(t[-1] for t in table) == pytest.approx(ms)
+    assert {t[3] for t in table} == {0, 1, 2, 4}
     # the tuner leaves the starting images alone
     for k, w in enumerate(ws):
         np.testing.assert_array_equal(batch.get_image(k), np.ones(w.vol.shape_zyx, np.float32))
