@@ -26,6 +26,9 @@ FIR_OPT_BLOCK_SIZE = 4
 FIR_OPT_TIMING = 5
 FIR_OPT_DETERMINISTIC_CHUNK = 6
 FIR_OPT_STEP_LIMIT = 7
+FIR_OPT_TRAVERSAL = 8
+FIR_TRAVERSAL_EXACT = 0
+FIR_TRAVERSAL_FLOAT = 1
 FIR_GEOMETRY_REFERENCE = 0
 FIR_GEOMETRY_EXACT = 1
 FIR_BACKPROJ_ATOMIC = 0

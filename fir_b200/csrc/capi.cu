@@ -534,6 +534,32 @@ void backproject_subset(fir_ctx& c, const Grid& g, const Sino& s, const Tables& 
 void ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, const float* img,
                        const float* sino, const float* mult, const float* bias, float* bp, long long nvox)
 {
+  if (c.traversal == FIR_TRAVERSAL_FLOAT && c.backproj == FIR_BACKPROJ_ATOMIC && mult == nullptr &&
+      c.step_limit == 0)
+  {
+    // the opt-in float loop: float images in both orientations while they
+    // and the accumulators fit in L2 (16 B per voxel)
+    const size_t n = (size_t)nvox;
+    float* img_t = nullptr;
+    float* bp_t = nullptr;
+    if (use_exchanged(c, g, 16.0))
+    {
+      img_t = static_cast<float*>(c.img_t.ensure(n * sizeof(float)));
+      bp_t = static_cast<float*>(c.bp_t.ensure(n * sizeof(float)));
+      cuda_ok(cudaMemsetAsync(bp_t, 0, n * sizeof(float), c.stream), "cudaMemsetAsync");
+      launch_exchange_float(g.nx, g.ny, g.nz, img, img_t, cfg_of(c));
+      after_launch(c);
+    }
+    timed_launch(c, [&] {
+      launch_osem_subset_float(g, s, t, img, img_t, sino, bias, bp, bp_t, c.skip_zero != 0, cfg_of(c));
+    });
+    if (bp_t != nullptr)
+    {
+      launch_merge_oriented(g.nx, g.ny, g.nz, bp, bp_t, cfg_of(c));
+      after_launch(c);
+    }
+    return;
+  }
   if (c.backproj == FIR_BACKPROJ_DETERMINISTIC)
   {
     const double* wimg = widen(c, img, nvox);
@@ -1425,6 +1451,13 @@ fir_status fir_ctx_set_option(fir_ctx* ctx, fir_option opt, int value)
       }
       c.step_limit = value;
       break;
+    case FIR_OPT_TRAVERSAL:
+      if (value != FIR_TRAVERSAL_EXACT && value != FIR_TRAVERSAL_FLOAT)
+      {
+        fail(FIR_ERR_INVALID_ARGUMENT, "unknown traversal mode ", value);
+      }
+      c.traversal = value;
+      break;
     case FIR_OPT_DETERMINISTIC_CHUNK:
       if (value < 0)
       {
@@ -1477,6 +1510,7 @@ fir_status fir_ctx_get_option(fir_ctx* ctx, fir_option opt, int* value)
     case FIR_OPT_TIMING: *value = c.timing ? 1 : 0; break;
     case FIR_OPT_DETERMINISTIC_CHUNK: *value = (int)std::min<long long>(c.det_chunk, 0x7fffffff); break;
     case FIR_OPT_STEP_LIMIT: *value = c.step_limit; break;
+    case FIR_OPT_TRAVERSAL: *value = c.traversal; break;
     default: fail(FIR_ERR_INVALID_ARGUMENT, "unknown option ", (int)opt);
     }
   });

@@ -47,6 +47,11 @@ void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const dou
 void launch_osem_subset_float_image(const Grid& g, const Sino& s, const Tables& t, const float* img,
                                     const float* sino, const float* mult, const float* bias, float* bp,
                                     bool skip_zero, const LaunchCfg& cfg);
+// fast.cu: the opt-in float traversal of the fused OSEM kernel.
+void launch_osem_subset_float(const Grid& g, const Sino& s, const Tables& t, const float* img, const float* img_t,
+                              const float* sino, const float* bias, float* bp, float* bp_t, bool skip_zero,
+                              const LaunchCfg& cfg);
+void launch_exchange_float(int nx, int ny, int nz, const float* in, float* out_t, const LaunchCfg& cfg);
 void launch_siddon_paths(const Grid& g, long long n, const double* ends, int cap, int* coords,
                          double* lengths, int* counts, int* crosses, const LaunchCfg& cfg);
 void launch_lor_paths(const Grid& g, const Sino& s, const Tables& t, long long n,

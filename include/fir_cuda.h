@@ -163,7 +163,17 @@ typedef enum fir_option
    * the call reports FIR_ERR_DEVICE_CHECK (host buffers) or the next
    * fir_ctx_synchronize does.  Results past the bound are truncated.  0
    * (default): the natural bound, which only non-finite input can reach. */
-  FIR_OPT_STEP_LIMIT = 7
+  FIR_OPT_STEP_LIMIT = 7,
+  /* FIR_TRAVERSAL_EXACT (default): FIR's double-precision traversal, voxel
+   * lists and lengths bit-identical to FIR's.  FIR_TRAVERSAL_FLOAT (opt-in,
+   * no counterpart in FIR): FIR's double set-up, then the loop in float with
+   * float accumulation, for the OSEM sub-iteration's projection and
+   * backprojection (fir_osem_subiteration, fir_osem, fir_ratio_backprojection
+   * in the atomic backprojection mode).  It changes the voxel lists of a few
+   * per cent of LORs (2.9 % of the clinical workload's) and line integrals by
+   * up to about 1 %; OSEM images stay within 1e-4 relative L2 of the exact
+   * mode's on the tested workloads.  The other projectors stay exact. */
+  FIR_OPT_TRAVERSAL = 8
 } fir_option;
 
 enum
@@ -171,7 +181,9 @@ enum
   FIR_GEOMETRY_REFERENCE = 0,
   FIR_GEOMETRY_EXACT = 1,
   FIR_BACKPROJ_ATOMIC = 0,
-  FIR_BACKPROJ_DETERMINISTIC = 1
+  FIR_BACKPROJ_DETERMINISTIC = 1,
+  FIR_TRAVERSAL_EXACT = 0,
+  FIR_TRAVERSAL_FLOAT = 1
 };
 
 /* ---- library / host helpers (no GPU needed) ---- */
