@@ -28,13 +28,18 @@ struct WalkF
 {
   float a[3], da[3];
   int step[3], left[3];
-  int c;
+  int c, tr;
   float amin, amax, d12;
+  float end;  // below this minimum no index can leave the volume
 };
 
+// The float state of a walk from FIR's double set-up.  end: every
+// dimension's exit crossing a + left * da, computed in double, less EPS and
+// a margin of 2^-10 for the rounding of the float running sums.
 __device__ __forceinline__ WalkF to_float(const Walk& w)
 {
   WalkF f;
+  double end = w.amax;
 #pragma unroll
   for (int d = 0; d < 3; ++d)
   {
@@ -42,42 +47,91 @@ __device__ __forceinline__ WalkF to_float(const Walk& w)
     f.da[d] = (float)w.da[d];
     f.step[d] = w.step[d];
     f.left[d] = w.left[d];
+    const double x = w.left[d] > 0 ? dadd(w.a[d], dmul((double)w.left[d], w.da[d])) : w.a[d];
+    const double lim = dsub(dsub(x, kEps), dmul(x, 0x1p-10));
+    end = (lim < end || lim != lim) ? lim : end;
   }
   f.c = w.c;
+  f.tr = w.tr;
   f.amin = (float)w.amin;
   f.amax = (float)w.amax;
   f.d12 = (float)w.d12;
+  f.end = (float)end;
   return f;
 }
 
-// The computePath loop (Siddon.cc:207-252) in float.  Every step emits the
-// current voxel (its index is inside the volume), advances each dimension
-// whose crossing lies within 1e-5 of the next alpha, and stops at alphaMax,
-// when an index leaves the volume, or at the step bound (only non-finite
-// input reaches it; the return value is then false).
+// Advances left in each dimension, from the linear index.
+__device__ __forceinline__ void left_from_index(const Grid& g, WalkF& w)
+{
+  const int z = w.c / g.nxy;
+  const int rest = w.c - z * g.nxy;
+  const int slow = rest / (w.tr ? g.ny : g.nx);
+  const int fast = rest - slow * (w.tr ? g.ny : g.nx);
+  const int idx[3] = {w.tr ? slow : fast, w.tr ? fast : slow, z};
+  const int n[3] = {g.nx, g.ny, g.nz};
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    w.left[d] = w.step[d] > 0 ? n[d] - 1 - idx[d] : idx[d];
+  }
+}
+
+// One step of the computePath loop (Siddon.cc:207-252) in float: emits the
+// current voxel (its index is inside the volume) and advances each dimension
+// whose crossing lies within 1e-5 of the next alpha.  Returns next alpha.
+template<bool kCount, class Emit>
+__device__ __forceinline__ float step_float(WalkF& w, float prev, Emit&& emit)
+{
+  const float m = fminf(w.a[0], fminf(w.a[1], w.a[2]));
+  const float next = fminf(m, w.amax);
+  emit(w.c, __fmul_rn(__fsub_rn(next, prev), w.d12));
+  const float thr = __fadd_rn(next, 1e-5f);
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    if (w.a[d] < thr)
+    {
+      w.a[d] = __fadd_rn(w.a[d], w.da[d]);
+      w.c += w.step[d];
+      if (kCount)
+      {
+        w.left[d] -= 1;
+      }
+    }
+  }
+  return next;
+}
+
+// The loop, stopping at alphaMax, when an index leaves the volume, or at
+// the step bound (only non-finite input reaches it; the return value is
+// then false).  As in the exact traversal, the steps below w.end run first
+// without the advance counts, which are then rebuilt from the voxel index for
+// the checked steps that end the walk.
 template<class Emit>
 __device__ __forceinline__ bool walk_float(const Grid& g, WalkF w, bool go, Emit&& emit)
 {
   float prev = w.amin;
-  bool more = go && prev < w.amax;
+  const bool active = go && prev < w.amax;
   int guard = g.guard;
+  if (active)
+  {
+    while (fminf(w.a[0], fminf(w.a[1], w.a[2])) < w.end && guard > 0)
+    {
+      prev = step_float<false>(w, prev, emit);
+      if (!(fminf(w.a[0], fminf(w.a[1], w.a[2])) < w.end))
+      {
+        break;
+      }
+      prev = step_float<false>(w, prev, emit);
+      guard -= 2;
+    }
+    left_from_index(g, w);
+  }
+  bool more = active;
   while (more)
   {
     const float m = fminf(w.a[0], fminf(w.a[1], w.a[2]));
-    const float next = fminf(m, w.amax);
-    emit(w.c, __fmul_rn(__fsub_rn(next, prev), w.d12));
-    const float thr = __fadd_rn(next, 1e-5f);
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-    {
-      if (w.a[d] < thr)
-      {
-        w.a[d] = __fadd_rn(w.a[d], w.da[d]);
-        w.c += w.step[d];
-        w.left[d] -= 1;
-      }
-    }
-    prev = next;
+    prev = step_float<true>(w, prev, emit);
     --guard;
     more = m < w.amax && (w.left[0] | w.left[1] | w.left[2]) >= 0 && guard > 0;
   }
