@@ -400,6 +400,7 @@ def batched_section(args, local):
         got = batch.get_image(k)
         want = imgs[k].cpu().numpy()
         err = max(err, float(np.linalg.norm(got - want) / max(np.linalg.norm(want), 1e-30)))
+    axial_tile = batch.bundle()
     batch.close()
     for c in plain_ctx:
         c.close()
@@ -420,7 +421,7 @@ def batched_section(args, local):
         "gpu_launches": launches,
         "plain_gpu_launches": plain_launches,
         "launch_shape": {"block": shape[0], "blocks_per_sm": shape[1], "grab": shape[2],
-                         "axial_tile": batch.bundle()},
+                         "axial_tile": axial_tile},
         "tuner_best_step0_ms": tune_ms,
         "tuner_candidates": [{"block": b, "blocks_per_sm": p, "grab": gr, "axial_tile": at, "step0_ms": round(t, 4)}
                              for b, p, gr, at, t in tune_table],
@@ -507,8 +508,13 @@ def autograd_section(args, local):
             xp, xm = xd.detach().clone(), xd.detach().clone()
             xp[j] += h
             xm[j] -= h
-            fd = (float(fa.penalized_nll(xp, y64, op, beta, a64)) - float(fa.penalized_nll(xm, y64, op, beta, a64))) \
-                / (2 * h)
+            # the loss difference summed bin by bin: the totals (~1e9) would
+            # carry rounding errors of ~1e-6 each
+            tp = fa.expected_counts(xp, op, a64)
+            tm = fa.expected_counts(xm, op, a64)
+            dl = float(((tp - torch.xlogy(y64, tp)) - (tm - torch.xlogy(y64, tm))).sum())
+            dl += float(fa.quadratic_penalty(xp, beta) - fa.quadratic_penalty(xm, beta))
+            fd = dl / (2 * h)
             fd_worst = max(fd_worst, abs(fd - float(gd[j])) / max(abs(float(gd[j])), 1e-3))
     del xd, gd, a64, y64
 
