@@ -422,7 +422,23 @@ __device__ __forceinline__ void left_from_index(const Grid& g, Walk& w)
 // X_d - EPS - X_d 2^-20 for every d, and next < alphaMax, no index leaves
 // and next is the minimum alpha.  Those steps run first without the
 // bookkeeping; the advance counts are then rebuilt from the linear index
-// and the checked steps finish the walk.  Two steps per trip in both.
+// and the checked steps finish the walk.
+//
+// The unchecked steps run in pairs behind one test.  A step moves the
+// minimum by at most the largest step `big` of the dimensions whose next
+// crossing lies below 1 (the one attaining the minimum advances by its
+// step, rounded; the others stay), and a dimension whose crossing is at or
+// beyond 1 never attains a minimum below end <= alphaMax <= 1 again, since
+// alphas only grow.  So a pair whose first minimum lies below end - big -
+// 4 EPS has its second one below end too.  The steps left before end run
+// singly.
+//
+// A dimension advances by adding a selected addend: its step when the tie
+// test holds, else the subnormal double whose low word is the step's (its
+// high word zeroed), which rounding absorbs: rn(a + s) = a for every alpha
+// of these steps (a >= EPS, s < 2^-1042).  The running sums are therefore
+// FIR's, and one select of a 32-bit word replaces the compiler's select of
+// both words of a conditionally added alpha.
 template<class Emit>
 __device__ __forceinline__ void walk_loop_fast(const Grid& g, Walk& w, double& prev, bool active, Emit&& emit)
 {
@@ -436,42 +452,47 @@ __device__ __forceinline__ void walk_loop_fast(const Grid& g, Walk& w, double& p
   }
   if (active)
   {
+    double big = 0.0;
+    int da_hi[3], da_lo[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+      big = (w.a[d] < 1.0 && w.da[d] > big) ? w.da[d] : big;
+      da_hi[d] = __double2hiint(w.da[d]);
+      da_lo[d] = __double2loint(w.da[d]);
+    }
+    const double end2 = dsub(dsub(end, big), 4.0 * kEps);
+    // one unchecked step from prev (its minimum m is below end)
+    auto step = [&](double m) {
+      emit(true, w.c, dmul(dsub(m, prev), w.d12));
+      const double thr = __dadd_ru(m, kEps);
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+      {
+        const bool p = w.a[d] < thr;
+        w.a[d] = dadd(w.a[d], __hiloint2double(p ? da_hi[d] : 0, da_lo[d]));
+        w.c += p ? w.step[d] : 0;
+      }
+      prev = m;
+    };
     while (true)
     {
-      double m = min_of(w.a[0], min_of(w.a[1], w.a[2]));
+      const double m = min_of(w.a[0], min_of(w.a[1], w.a[2]));
+      if (!(m < end2))
+      {
+        break;
+      }
+      step(m);
+      step(min_of(w.a[0], min_of(w.a[1], w.a[2])));
+    }
+    while (true)
+    {
+      const double m = min_of(w.a[0], min_of(w.a[1], w.a[2]));
       if (!(m < end))
       {
         break;
       }
-      emit(true, w.c, dmul(dsub(m, prev), w.d12));
-      double thr = __dadd_ru(m, kEps);
-#pragma unroll
-      for (int d = 0; d < 3; ++d)
-      {
-        if (w.a[d] < thr)
-        {
-          w.a[d] = dadd(w.a[d], w.da[d]);
-          w.c += w.step[d];
-        }
-      }
-      prev = m;
-      m = min_of(w.a[0], min_of(w.a[1], w.a[2]));
-      if (!(m < end))
-      {
-        break;
-      }
-      emit(true, w.c, dmul(dsub(m, prev), w.d12));
-      thr = __dadd_ru(m, kEps);
-#pragma unroll
-      for (int d = 0; d < 3; ++d)
-      {
-        if (w.a[d] < thr)
-        {
-          w.a[d] = dadd(w.a[d], w.da[d]);
-          w.c += w.step[d];
-        }
-      }
-      prev = m;
+      step(m);
     }
     left_from_index(g, w);
   }
