@@ -172,7 +172,19 @@ __global__ void __launch_bounds__(256, 4) k_osem_subset_float(Grid g, Sino s, Ta
   float* b = tr ? bp_t : bp;
   __builtin_assume(__isGlobal(b));
   float line = 0.0f;
-  bool ok = walk_float(g, wf, go, [&](int c, float len) { line = __fmaf_rn(len, __ldg(im + c), line); });
+  // each gather is issued two steps before its value is accumulated, so its
+  // latency overlaps the walk of those steps; the sum is the same, term by
+  // term in order
+  float l0 = 0.0f, v0 = 0.0f, l1 = 0.0f, v1 = 0.0f;
+  bool ok = walk_float(g, wf, go, [&](int c, float len) {
+    line = __fmaf_rn(l0, v0, line);
+    l0 = l1;
+    v0 = v1;
+    l1 = len;
+    v1 = __ldg(im + c);
+  });
+  line = __fmaf_rn(l0, v0, line);
+  line = __fmaf_rn(l1, v1, line);
   __syncwarp();
   if (valid && bias != nullptr)
   {
