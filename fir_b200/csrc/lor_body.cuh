@@ -69,13 +69,20 @@ __device__ __forceinline__ void osem_lor_body(const Grid& g, const Sino& s, int 
   // this the compiler cannot tell the atomic's address space and tests it at
   // every step.
   __builtin_assume(__isGlobal(b));
+  // Each gather is issued one step before its term is accumulated, so its
+  // latency overlaps a step of the walk.  The terms are added in the same
+  // order; the first call adds 0 * 0 to the zero sum, which leaves it 0.
   float line = 0.0f;
+  double pl = 0.0, pv = 0.0;
   bool ok = siddon_walk(g, w, go, [&](bool inside, int c, double len) {
     if (inside)
     {
-      line = accumulate(line, len, (double)__ldg(im + c));
+      line = accumulate(line, pl, pv);
+      pl = len;
+      pv = (double)__ldg(im + c);
     }
   });
+  line = accumulate(line, pl, pv);
   __syncwarp();
   const float m = kWeighted && valid ? __ldg(mult + l.bin) : 1.0f;
   if (kWeighted)
