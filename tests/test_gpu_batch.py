@@ -144,6 +144,17 @@ def test_bundle_shapes_agree(tile, shape):
     ctx.close()
 
 
+def test_bundle_shape_checked():
+    ws = mixed_problems()[:1]
+    ctx, batch, data = build(ws, bias_for=())
+    for bad in (3, 16, -1):
+        with pytest.raises(capi.FirError, match="axial tile"):
+            batch.set_bundle(bad)
+    assert batch.bundle() == 0
+    batch.close()
+    ctx.close()
+
+
 def test_tuner_keeps_images_and_results(restated):
     ws = mixed_problems()[:2]
     ctx, batch, data = build(ws, bias_for=())

@@ -139,3 +139,13 @@ def test_cpp_reso_reco_dropin_matches_fir(case, tmp_path):
     _, got_sens = interfile.read_vol(str(d / "out_sens.h33"))
     np.testing.assert_array_equal(got_sens.ravel(), sens_ref)
     assert rel_l2(got, img_ref) <= 1e-4
+
+
+def test_abi_reso_reco_rejects_too_few_sensitivity_frames(case):
+    """FIR's setActiveFrame(subset) fails with "Invalid frame" when the
+    sensitivity volume has fewer frames than subsets."""
+    w, x, y, sens, bias, img_ref, sens_ref = case
+    with capi.Context(w.scanner) as ctx:
+        img = np.ones(w.vol.shape_zyx, np.float32)
+        with pytest.raises(capi.FirError, match="Invalid frame"):
+            ctx.osem_reso_reco(w.proj, y, w.vol, img, sens.copy(), PRM, n_sens_frames=3)

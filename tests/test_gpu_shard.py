@@ -68,3 +68,19 @@ def test_sharded_osem_one_rank_is_fir_osem():
         ShardedOSEM(ctx, w.proj, w.vol, prm).run(y, b, sens)
         torch.cuda.synchronize()
         np.testing.assert_array_equal(a.cpu().numpy(), b.cpu().numpy())
+
+
+def test_shard_arguments_checked():
+    import torch
+
+    w = workloads.small()
+    with capi.Context(w.scanner) as ctx:
+        nb = capi.proj_geometry(w.proj)["n_bins"]
+        y = torch.ones(nb, device="cuda")
+        img = torch.ones(w.vol.shape_zyx, device="cuda")
+        bp = torch.empty_like(img)
+        for n_shards, shard in ((0, 0), (3, 3), (3, -1)):
+            with pytest.raises(capi.FirError, match="shard"):
+                ctx.ratio_backprojection(w.proj, y, w.vol, img, bp, 4, 1, n_shards=n_shards, shard=shard)
+        with pytest.raises(capi.FirError):
+            ctx.ratio_backprojection(w.proj, y, w.vol, img, bp, 5, 1, n_shards=2, shard=0)  # 5 does not divide 64 views
