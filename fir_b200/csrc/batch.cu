@@ -80,10 +80,10 @@ __device__ __forceinline__ int tiled_lor(const Sino& s, const int* __restrict__ 
   return s.enum_base[lo] + (sv * nax + a) * s.n_tang + t;
 }
 
-// TImg: what the projection gathers from, each problem's double copy or (for
-// problems whose double copy does not fit in L2 beside the accumulator) its
-// float image.  A launch covers problems of one kind.
-template<bool kPersistent, typename TImg>
+// The projection gathers each problem's double copy.  Problems whose volumes
+// fit L2 only as float image and accumulator run fir_osem's kernel in launches
+// of their own instead.
+template<bool kPersistent>
 __global__ void __launch_bounds__(256, 4) k_batch_osem(const BatchProblem* __restrict__ P,
                                                     const BatchItem* __restrict__ items, int n_items,
                                                     int n_bundles, int* queue, int grab, int axial_tile,
@@ -103,16 +103,8 @@ __global__ void __launch_bounds__(256, 4) k_batch_osem(const BatchProblem* __res
       const BatchProblem& pb = P[p];
       const int j = k - __ldg(&items[it].unit_begin);
       const int i = axial_tile == 0 ? j * 32 + lane : tiled_lor(pb.s, pb.bundle_base, j, axial_tile, lane);
-      if constexpr (sizeof(TImg) == sizeof(double))
-      {
-        osem_lor(pb.g, pb.s, subset, pb.t, pb.wide, pb.wide_t, pb.sino, pb.bias, pb.bp, pb.bp_t, pb.skip_zero != 0,
-                 i, check);
-      }
-      else
-      {
-        osem_lor_body<false, float>(pb.g, pb.s, subset, pb.t, pb.img, nullptr, pb.sino, nullptr, pb.bias, pb.bp,
-                                    nullptr, pb.skip_zero != 0, i, check);
-      }
+      osem_lor(pb.g, pb.s, subset, pb.t, pb.wide, pb.wide_t, pb.sino, pb.bias, pb.bp, pb.bp_t, pb.skip_zero != 0, i,
+               check);
       // lanes whose paths ended early wait here, so that the warp starts the
       // next bundle together instead of splitting across two bundles
       __syncwarp();
@@ -188,10 +180,17 @@ __global__ void __launch_bounds__(kBatchBlock) k_batch_prepare(const BatchProble
     pb.wide[v.j] = (double)x;
   }
   pb.bp[v.j] = 0.0f;
-  if (pb.wide_t != nullptr)
+  if (pb.bp_t != nullptr)
   {
     const int jt = exchanged(pb, v.j);
-    pb.wide_t[jt] = (double)x;
+    if (pb.wide_t != nullptr)
+    {
+      pb.wide_t[jt] = (double)x;
+    }
+    if (pb.img_t != nullptr)
+    {
+      pb.img_t[jt] = x;
+    }
     pb.bp_t[jt] = 0.0f;
   }
 }
@@ -229,9 +228,13 @@ __global__ void __launch_bounds__(kBatchBlock) k_batch_em(const BatchProblem* __
     {
       pb.wide[v.j] = (double)x;
     }
-    if (jt >= 0)
+    if (jt >= 0 && pb.wide_t != nullptr)
     {
       pb.wide_t[jt] = (double)x;
+    }
+    if (jt >= 0 && pb.img_t != nullptr)
+    {
+      pb.img_t[jt] = x;
     }
   }
   pb.img[v.j] = x;
@@ -309,6 +312,10 @@ __global__ void __launch_bounds__(kBatchBlock) k_batch_filter(const BatchProblem
     {
       pb.wide_t[exchanged(pb, j)] = (double)x;
     }
+    if (pb.img_t != nullptr)
+    {
+      pb.img_t[exchanged(pb, j)] = x;
+    }
   }
 }
 }  // namespace
@@ -324,7 +331,6 @@ void launch_batch_prepare(const BatchProblem* P, const BatchItem* items, int n_i
 
 namespace
 {
-template<typename TImg>
 void project(const BatchProblem* P, const BatchItem* items, int n_items, int n_bundles, int* queue,
              const BatchLaunch& L, int n_sms, int* check, cudaStream_t stream)
 {
@@ -332,8 +338,8 @@ void project(const BatchProblem* P, const BatchItem* items, int n_items, int n_b
   const long long plain_blocks = (threads + L.block - 1) / L.block;
   if (L.blocks_per_sm <= 0)
   {
-    k_batch_osem<false, TImg><<<(unsigned)plain_blocks, L.block, 0, stream>>>(P, items, n_items, n_bundles,
-                                                                               nullptr, 1, L.axial_tile, check);
+    k_batch_osem<false><<<(unsigned)plain_blocks, L.block, 0, stream>>>(P, items, n_items, n_bundles, nullptr, 1,
+                                                                         L.axial_tile, check);
     return;
   }
   long long blocks = (long long)n_sms * L.blocks_per_sm;
@@ -341,27 +347,19 @@ void project(const BatchProblem* P, const BatchItem* items, int n_items, int n_b
   {
     blocks = plain_blocks;
   }
-  k_batch_osem<true, TImg><<<(unsigned)blocks, L.block, 0, stream>>>(P, items, n_items, n_bundles, queue, L.grab,
-                                                                      L.axial_tile, check);
+  k_batch_osem<true><<<(unsigned)blocks, L.block, 0, stream>>>(P, items, n_items, n_bundles, queue, L.grab,
+                                                                L.axial_tile, check);
 }
 }  // namespace
 
 void launch_batch_project(const BatchProblem* P, const BatchItem* items, int n_items, int n_bundles,
-                          int* queue, const BatchLaunch& L, int n_sms, int* check, bool gather_float,
-                          cudaStream_t stream)
+                          int* queue, const BatchLaunch& L, int n_sms, int* check, cudaStream_t stream)
 {
   if (n_bundles <= 0)
   {
     return;
   }
-  if (gather_float)
-  {
-    project<float>(P, items, n_items, n_bundles, queue, L, n_sms, check, stream);
-  }
-  else
-  {
-    project<double>(P, items, n_items, n_bundles, queue, L, n_sms, check, stream);
-  }
+  project(P, items, n_items, n_bundles, queue, L, n_sms, check, stream);
 }
 
 void launch_batch_em(const BatchProblem* P, const BatchItem* items, int n_items, int n_units, cudaStream_t stream)
@@ -426,7 +424,7 @@ void batch_bundle_bases(const Sino& s, int axial_tile, int* base)
 int batch_max_resident(int block)
 {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_osem<true, double>, block, 0) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_osem<true>, block, 0) != cudaSuccess)
   {
     cudaGetLastError();
     return 1;

@@ -576,10 +576,20 @@ void ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t
     if (!use_exchanged(c, g, 12.0) && use_exchanged(c, g, 8.0))
     {
       // the double copy and the accumulator (12 B/voxel) overflow L2, the
-      // float image and the accumulator (8 B/voxel) fit: gather floats
+      // float image and the accumulator (8 B/voxel) fit: gather floats, one
+      // launch per orientation, each with its own image and accumulator
+      const size_t n = (size_t)nvox;
+      float* img_t = static_cast<float*>(c.img_t.ensure(n * sizeof(float)));
+      float* bp_t = static_cast<float*>(c.bp_t.ensure(n * sizeof(float)));
+      cuda_ok(cudaMemsetAsync(bp_t, 0, n * sizeof(float), c.stream), "cudaMemsetAsync");
+      launch_exchange_float(g.nx, g.ny, g.nz, img, img_t, cfg_of(c));
+      after_launch(c);
       timed_launch(c, [&] {
-        launch_osem_subset_float_image(g, s, t, img, sino, mult, bias, bp, c.skip_zero != 0, cfg_of(c));
+        launch_osem_subset_float_image(g, s, t, img, img_t, sino, mult, bias, bp, bp_t, c.skip_zero != 0,
+                                       cfg_of(c));
       });
+      launch_merge_oriented(g.nx, g.ny, g.nz, bp, bp_t, cfg_of(c));
+      after_launch(c);
       return;
     }
     const double* wimg = widen(c, img, nvox);

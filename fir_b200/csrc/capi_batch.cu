@@ -20,6 +20,17 @@ using namespace fir::abi;
 //             filter items (voxel blocks of the problems that filter at t)
 // Items of the projector are ordered by decreasing path length, so that the
 // queue hands out the longest bundles first.
+//
+// A problem whose subsets alone fill the GPU many times over (kDirectLors),
+// or whose volume fits L2 only as float image and accumulator, runs its
+// projector as fir_osem does, in launches of its own within the step: the
+// kernel then reads its descriptor from kernel parameters rather than from
+// memory, which leaves the walk the registers it needs (the large 320x320x128
+// problem: 358 ms of projector per iteration batched, 325 ms direct), and the
+// float gathers run as one launch per orientation.
+
+// 2^22 LORs per subset: 14 waves of 148 SMs x 2048 threads.
+constexpr long long kDirectLors = 1LL << 22;
 
 struct fir_batch
 {
@@ -34,9 +45,12 @@ struct fir_batch
     bool filter = false;
     bool exchanged = false;  // x/y-exchanged images for LORs along x (use_exchanged)
     bool gather_float = false;  // no double copy: too large for L2 beside the accumulator
+    // the projector runs as fir_osem's kernel in launches of its own, its
+    // descriptor as kernel parameters (kDirectLors)
+    bool direct = false;
     double path = 0.0;  // nx + ny + nz: relative cost of a bundle
     size_t off_sino = 0, off_sens = 0, off_img = 0, off_wide = 0, off_bp = 0, off_wide_t = 0, off_bp_t = 0,
-           off_t1 = 0, off_t2 = 0, off_xy = 0, off_z = 0;
+           off_img_t = 0, off_t1 = 0, off_t2 = 0, off_xy = 0, off_z = 0;
     DevBuf bias;
   };
   struct Launch
@@ -45,7 +59,8 @@ struct fir_batch
   };
   struct Step
   {
-    Launch proj, proj_f, em, filt;  // proj_f: problems that gather their float images
+    Launch proj, em, filt;
+    std::vector<std::pair<int, int>> direct;  // (problem, subset) of the direct projector launches
   };
 
   fir_ctx* ctx = nullptr;
@@ -155,15 +170,33 @@ void check_launch(cudaStream_t s)
   cuda_ok(cudaGetLastError(), "kernel launch");
 }
 
-// Enqueues one projector launch of a step (queue: its zeroed counter).
-void batch_project(fir_batch& b, const fir_batch::Launch& L, int* queue, const BatchLaunch& shape, bool gather_float,
-                   cudaStream_t s)
+// Enqueues the batched projector launch of a step (queue: its zeroed counter).
+void batch_project(fir_batch& b, const fir_batch::Launch& L, int* queue, const BatchLaunch& shape, cudaStream_t s)
 {
   const auto* P = static_cast<const BatchProblem*>(b.desc.p);
   const auto* I = static_cast<const BatchItem*>(b.items.p) + L.item_off;
-  launch_batch_project(P, I, L.n_items, L.n_units, queue, shape, b.n_sms, static_cast<int*>(b.ctx->check.p),
-                       gather_float, s);
+  launch_batch_project(P, I, L.n_items, L.n_units, queue, shape, b.n_sms, static_cast<int*>(b.ctx->check.p), s);
   check_launch(s);
+}
+
+// Enqueues problem k's projector for one subset as fir_osem runs it (one
+// launch, two when it gathers floats); returns the number of launches.
+long long direct_project(fir_batch& b, int k, int subset, cudaStream_t s)
+{
+  const BatchProblem& d = b.desc_host[(size_t)k];
+  Sino sub = d.s;
+  sub.subset = subset;
+  const LaunchCfg cfg{b.ctx->block, s, static_cast<int*>(b.ctx->check.p)};
+  if (b.pr[(size_t)k].gather_float)
+  {
+    launch_osem_subset_float_image(d.g, sub, d.t, d.img, d.img_t, d.sino, nullptr, d.bias, d.bp, d.bp_t,
+                                   d.skip_zero != 0, cfg);
+    check_launch(s);
+    return d.img_t != nullptr ? 2 : 1;
+  }
+  launch_osem_subset(d.g, sub, d.t, d.wide, d.wide_t, d.sino, nullptr, d.bias, d.bp, d.bp_t, d.skip_zero != 0, cfg);
+  check_launch(s);
+  return 1;
 }
 
 // The whole schedule on stream s; returns the number of kernel launches.
@@ -173,19 +206,18 @@ long long batch_enqueue(fir_batch& b, cudaStream_t s)
   const auto* I = static_cast<const BatchItem*>(b.items.p);
   int* queue = static_cast<int*>(b.queue.p);
   long long n = 0;
-  cuda_ok(cudaMemsetAsync(queue, 0, 2 * b.steps.size() * sizeof(int), s), "cudaMemsetAsync");
+  cuda_ok(cudaMemsetAsync(queue, 0, b.steps.size() * sizeof(int), s), "cudaMemsetAsync");
   launch_batch_prepare(P, I + b.all.item_off, b.all.n_items, b.all.n_units, true, s);
   check_launch(s);
   ++n;
   for (size_t t = 0; t < b.steps.size(); ++t)
   {
     const fir_batch::Step& st = b.steps[t];
-    batch_project(b, st.proj, queue + 2 * t, b.shape, false, s);
+    batch_project(b, st.proj, queue + t, b.shape, s);
     n += st.proj.n_items > 0 ? 1 : 0;
-    if (st.proj_f.n_items > 0)
+    for (const auto& ks : st.direct)
     {
-      batch_project(b, st.proj_f, queue + 2 * t + 1, b.shape, true, s);
-      ++n;
+      n += direct_project(b, ks.first, ks.second, s);
     }
     launch_batch_em(P, I + st.em.item_off, st.em.n_items, st.em.n_units, s);
     check_launch(s);
@@ -238,7 +270,8 @@ void build_schedule(fir_batch& b)
   }
   for (int t = 0; t < n_steps; ++t)
   {
-    std::vector<int> probs, subs, filts, fprobs, fsubs, fflags, dprobs, dsubs, dfilts, gprobs, gsubs, gfilts;
+    std::vector<int> probs, subs, filts, fprobs, fsubs, fflags, dprobs, dsubs, dfilts;
+    fir_batch::Step st;
     for (int k : order)
     {
       const fir_batch::Problem& q = b.pr[(size_t)k];
@@ -251,9 +284,16 @@ void build_schedule(fir_batch& b)
       probs.push_back(k);
       subs.push_back(t % q.n_subsets);
       filts.push_back(f);
-      (q.gather_float ? gprobs : dprobs).push_back(k);
-      (q.gather_float ? gsubs : dsubs).push_back(t % q.n_subsets);
-      (q.gather_float ? gfilts : dfilts).push_back(f);
+      if (q.direct)
+      {
+        st.direct.emplace_back(k, t % q.n_subsets);
+      }
+      else
+      {
+        dprobs.push_back(k);
+        dsubs.push_back(t % q.n_subsets);
+        dfilts.push_back(f);
+      }
       if (f)
       {
         fprobs.push_back(k);
@@ -261,9 +301,7 @@ void build_schedule(fir_batch& b)
         fflags.push_back(1);
       }
     }
-    fir_batch::Step st;
     st.proj = add_launch(items, dprobs, dsubs, dfilts, lor_units);
-    st.proj_f = add_launch(items, gprobs, gsubs, gfilts, lor_units);
     st.em = add_launch(items, probs, subs, filts, vox_units);
     st.filt = add_launch(items, fprobs, fsubs, fflags, vox_units);
     b.steps.push_back(st);
@@ -272,13 +310,17 @@ void build_schedule(fir_batch& b)
   batch_copy(b, b.desc.p, b.desc_host.data(), b.desc_host.size() * sizeof(BatchProblem));
   b.items.ensure(std::max<size_t>(items.size(), 1) * sizeof(BatchItem));
   batch_copy(b, b.items.p, items.data(), items.size() * sizeof(BatchItem));
-  b.queue.ensure(std::max<size_t>(2 * b.steps.size(), 1) * sizeof(int));
+  b.queue.ensure(std::max<size_t>(b.steps.size(), 1) * sizeof(int));
   cuda_ok(cudaStreamSynchronize(b.ctx->stream), "cudaStreamSynchronize");
   b.schedule_launches = 1;
   for (const auto& st : b.steps)
   {
-    b.schedule_launches += 1 + (st.proj.n_items > 0 ? 1 : 0) + (st.proj_f.n_items > 0 ? 1 : 0) +
-                           (st.filt.n_items > 0 ? 3 : 0);
+    b.schedule_launches += 1 + (st.proj.n_items > 0 ? 1 : 0) + (st.filt.n_items > 0 ? 3 : 0);
+    for (const auto& ks : st.direct)
+    {
+      const BatchProblem& d = b.desc_host[(size_t)ks.first];
+      b.schedule_launches += d.img_t != nullptr ? 2 : 1;
+    }
   }
 }
 
@@ -380,7 +422,8 @@ fir_status fir_batch_create(fir_batch** out, fir_ctx* ctx, int n_problems, const
       q.off_wide = take(q.gather_float ? 0 : nv * sizeof(double));
       q.off_bp = take(nv * sizeof(float));
       q.off_wide_t = take(q.exchanged ? nv * sizeof(double) : 0);
-      q.off_bp_t = take(q.exchanged ? nv * sizeof(float) : 0);
+      q.off_bp_t = take(q.exchanged || q.gather_float ? nv * sizeof(float) : 0);
+      q.off_img_t = take(q.gather_float ? nv * sizeof(float) : 0);
       q.off_t1 = take(q.filter ? nv * sizeof(float) : 0);
       q.off_t2 = take(q.filter ? nv * sizeof(float) : 0);
       q.off_xy = take(scan[(size_t)k].xy.size() * sizeof(double));
@@ -405,6 +448,7 @@ fir_status fir_batch_create(fir_batch** out, fir_ctx* ctx, int n_problems, const
         d.g = grid_of(geo, q.v);
         d.s = sino_of(q.p, q.n_subsets, 0);
         q.n_enum = d.s.n_enum;
+        q.direct = q.gather_float || (long long)q.n_enum >= kDirectLors;
         batch_copy(*b, base + q.off_xy, scan[(size_t)k].xy.data(), scan[(size_t)k].xy.size() * sizeof(double));
         batch_copy(*b, base + q.off_z, scan[(size_t)k].z.data(), scan[(size_t)k].z.size() * sizeof(double));
         d.t = Tables{reinterpret_cast<const double2*>(base + q.off_xy), reinterpret_cast<const double*>(base + q.off_z)};
@@ -415,7 +459,8 @@ fir_status fir_batch_create(fir_batch** out, fir_ctx* ctx, int n_problems, const
         d.wide = q.gather_float ? nullptr : reinterpret_cast<double*>(base + q.off_wide);
         d.bp = reinterpret_cast<float*>(base + q.off_bp);
         d.wide_t = q.exchanged ? reinterpret_cast<double*>(base + q.off_wide_t) : nullptr;
-        d.bp_t = q.exchanged ? reinterpret_cast<float*>(base + q.off_bp_t) : nullptr;
+        d.bp_t = q.exchanged || q.gather_float ? reinterpret_cast<float*>(base + q.off_bp_t) : nullptr;
+        d.img_t = q.gather_float ? reinterpret_cast<float*>(base + q.off_img_t) : nullptr;
         d.t1 = q.filter ? reinterpret_cast<float*>(base + q.off_t1) : nullptr;
         d.t2 = q.filter ? reinterpret_cast<float*>(base + q.off_t2) : nullptr;
         d.nvox = (int)q.v.nvox;
@@ -486,6 +531,8 @@ fir_status fir_batch_set_data(fir_batch* batch, int p, const float* sino, const 
     {
       d.bias = want;
       batch_copy(b, static_cast<BatchProblem*>(b.desc.p) + p, &d, sizeof(BatchProblem));
+      // a direct projector launch holds the bias pointer in its parameters
+      drop_graph(b);
     }
     cuda_ok(cudaStreamSynchronize(b.ctx->stream), "cudaStreamSynchronize");
   });
@@ -604,6 +651,20 @@ fir_status fir_batch_tune(fir_batch* batch, double* best_ms)
         *best_ms = 0.0;
       return;
     }
+    // the first step whose projector batches problems (direct launches do
+    // not use the shape)
+    size_t t0 = 0;
+    while (t0 < b.steps.size() && b.steps[t0].proj.n_items == 0)
+    {
+      ++t0;
+    }
+    if (t0 == b.steps.size())
+    {
+      b.tuned.clear();
+      if (best_ms != nullptr)
+        *best_ms = 0.0;
+      return;
+    }
     const BatchProblem* P = static_cast<const BatchProblem*>(b.desc.p);
     const BatchItem* I = static_cast<const BatchItem*>(b.items.p);
     int* queue = static_cast<int*>(b.queue.p);
@@ -658,10 +719,7 @@ fir_status fir_batch_tune(fir_batch* batch, double* best_ms)
           check_launch(b.stream);
           cuda_ok(cudaMemsetAsync(queue, 0, sizeof(int), b.stream), "cudaMemsetAsync");
           cuda_ok(cudaEventRecord(e0, b.stream), "cudaEventRecord");
-          // step 0's projector: the double-gather launch, or the float one
-          // when every problem gathers floats
-          const bool f = b.steps[0].proj.n_items == 0;
-          batch_project(b, f ? b.steps[0].proj_f : b.steps[0].proj, queue, L, f, b.stream);
+          batch_project(b, b.steps[t0].proj, queue, L, b.stream);
           cuda_ok(cudaEventRecord(e1, b.stream), "cudaEventRecord");
           cuda_ok(cudaEventSynchronize(e1), "cudaEventSynchronize");
           float ms = 0.0f;

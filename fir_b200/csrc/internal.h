@@ -43,10 +43,12 @@ void launch_backward(const Grid& g, const Sino& s, const Tables& t, const float*
 void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const double* img, const double* img_t,
                         const float* sino, const float* mult, const float* bias, float* bp, float* bp_t,
                         bool skip_zero, const LaunchCfg& cfg);
-// The same (one orientation), gathering from the float image itself.
+// The same, gathering from the float image itself; with the exchanged float
+// image and accumulator (img_t, bp_t, both or neither) as two launches, one
+// per orientation.
 void launch_osem_subset_float_image(const Grid& g, const Sino& s, const Tables& t, const float* img,
-                                    const float* sino, const float* mult, const float* bias, float* bp,
-                                    bool skip_zero, const LaunchCfg& cfg);
+                                    const float* img_t, const float* sino, const float* mult, const float* bias,
+                                    float* bp, float* bp_t, bool skip_zero, const LaunchCfg& cfg);
 // fast.cu: the opt-in float traversal of the fused OSEM kernel.
 void launch_osem_subset_float(const Grid& g, const Sino& s, const Tables& t, const float* img, const float* img_t,
                               const float* sino, const float* bias, float* bp, float* bp_t, bool skip_zero,
@@ -139,8 +141,12 @@ struct BatchProblem
   float* img;
   double* wide;  // double copy of img for the projector gathers (null: it gathers img itself)
   float* bp;
-  double* wide_t;  // wide and bp with x and y exchanged ([z][x][y]), for LORs
-  float* bp_t;     // running mostly along x; bp_t is added into bp by the EM step
+  // wide, img and bp with x and y exchanged ([z][x][y]), for LORs running
+  // mostly along x; bp_t is added into bp by the EM step.  Problems with the
+  // double copy have wide_t, those that gather floats img_t (null: none).
+  double* wide_t;
+  float* bp_t;
+  float* img_t;
   float* t1;
   float* t2;
   int nvox;
@@ -186,11 +192,10 @@ void batch_bundle_bases(const Sino& s, int axial_tile, int* base);
 void launch_batch_prepare(const BatchProblem* P, const BatchItem* items, int n_items, int n_units,
                           bool write_img, cudaStream_t stream);
 // bp += backprojection of measured/estimated for every item's subset.
-// queue: a zeroed counter (persistent mode).  gather_float: the items'
-// problems have no double copy (wide == null) and gather their float images.
+// queue: a zeroed counter (persistent mode).  The items' problems gather
+// their double copies (wide).
 void launch_batch_project(const BatchProblem* P, const BatchItem* items, int n_items, int n_bundles,
-                          int* queue, const BatchLaunch& L, int n_sms, int* check, bool gather_float,
-                          cudaStream_t stream);
+                          int* queue, const BatchLaunch& L, int n_sms, int* check, cudaStream_t stream);
 // Gated EM update of img; bp <- 0.  Items without filtering also apply the
 // cut and refresh wide.
 void launch_batch_em(const BatchProblem* P, const BatchItem* items, int n_items, int n_units,

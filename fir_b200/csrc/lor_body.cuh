@@ -31,7 +31,9 @@ __device__ __forceinline__ void flag(int* check, int bit)
 // y exchanged.  A LOR that runs mostly along x gathers from img_t and adds
 // into bp_t: the 32 parallel LORs of a warp are then offset along the
 // contiguous axis, so each warp-wide gather and atomic touches about half as
-// many cache lines.  The caller adds bp_t back into bp.
+// many cache lines.  The caller adds bp_t back into bp.  orient 0 (1) limits
+// the call to the LORs of the first (second, exchanged) orientation, so that
+// two launches each keep one orientation's images in L2; -1 takes both.
 //
 // TImg: the image the projection gathers from, the double copy or the float
 // image itself (widened per step, exact; for volumes whose double copy does
@@ -41,7 +43,7 @@ __device__ __forceinline__ void osem_lor_body(const Grid& g, const Sino& s, int 
                                               const TImg* __restrict__ img, const TImg* __restrict__ img_t,
                                               const float* __restrict__ sino, const float* __restrict__ mult,
                                               const float* __restrict__ bias, float* bp, float* bp_t,
-                                              bool skip_zero, int i, int* check)
+                                              bool skip_zero, int i, int* check, int orient = -1)
 {
   const bool valid = i < s.n_enum;
   Lor l{};
@@ -60,7 +62,11 @@ __device__ __forceinline__ void osem_lor_body(const Grid& g, const Sino& s, int 
       double e[6];
       lor_ends(s, t, l, e);
       tr = img_t != nullptr && fabs(dsub(e[3], e[0])) > fabs(dsub(e[4], e[1]));
-      go = siddon_setup(g, e, w, tr);
+      // orient 0 or 1: this launch takes only the LORs of that orientation
+      if (orient < 0 || (tr ? 1 : 0) == orient)
+      {
+        go = siddon_setup(g, e, w, tr);
+      }
     }
   }
   const TImg* im = tr ? img_t : img;

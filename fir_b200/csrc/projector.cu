@@ -121,11 +121,11 @@ __global__ void __launch_bounds__(256, 4) k_osem_subset(Grid g, Sino s, Tables t
                                                         const float* __restrict__ sino,
                                                         const float* __restrict__ mult,
                                                         const float* __restrict__ bias, float* bp, float* bp_t,
-                                                        int skip_zero, int* check)
+                                                        int skip_zero, int* check, int orient)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   osem_lor_body<kWeighted, TImg>(g, s, s.subset, t, img, img_t, sino, mult, bias, bp, bp_t, skip_zero != 0, i,
-                                 check);
+                                 check, orient);
 }
 
 // Path dump of one segment into row i of coords / lengths.
@@ -253,33 +253,43 @@ void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const dou
   if (mult != nullptr)
   {
     k_osem_subset<true, double><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, img_t, sino, mult, bias, bp, bp_t,
-                                                                  skip_zero ? 1 : 0, cfg.check);
+                                                                  skip_zero ? 1 : 0, cfg.check, -1);
   }
   else
   {
     k_osem_subset<false, double><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, img_t, sino, nullptr, bias, bp,
-                                                                   bp_t, skip_zero ? 1 : 0, cfg.check);
+                                                                   bp_t, skip_zero ? 1 : 0, cfg.check, -1);
   }
 }
 
 void launch_osem_subset_float_image(const Grid& g, const Sino& s, const Tables& t, const float* img,
-                                    const float* sino, const float* mult, const float* bias, float* bp,
-                                    bool skip_zero, const LaunchCfg& cfg)
+                                    const float* img_t, const float* sino, const float* mult, const float* bias,
+                                    float* bp, float* bp_t, bool skip_zero, const LaunchCfg& cfg)
 {
   if (s.n_enum == 0)
   {
     return;
   }
-  const unsigned nb = blocks_for(s.n_enum, cfg.block);
-  if (mult != nullptr)
+  if (img_t == nullptr || bp_t == nullptr)
   {
-    k_osem_subset<true, float><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, nullptr, sino, mult, bias, bp,
-                                                                 nullptr, skip_zero ? 1 : 0, cfg.check);
+    img_t = nullptr;
+    bp_t = nullptr;
   }
-  else
+  const unsigned nb = blocks_for(s.n_enum, cfg.block);
+  // with the exchanged images: one launch per orientation
+  const int first = img_t != nullptr ? 0 : -1, last = img_t != nullptr ? 1 : -1;
+  for (int o = first; o <= last; ++o)
   {
-    k_osem_subset<false, float><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, nullptr, sino, nullptr, bias, bp,
-                                                                  nullptr, skip_zero ? 1 : 0, cfg.check);
+    if (mult != nullptr)
+    {
+      k_osem_subset<true, float><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, img_t, sino, mult, bias, bp, bp_t,
+                                                                   skip_zero ? 1 : 0, cfg.check, o);
+    }
+    else
+    {
+      k_osem_subset<false, float><<<nb, cfg.block, 0, cfg.stream>>>(g, s, t, img, img_t, sino, nullptr, bias, bp,
+                                                                    bp_t, skip_zero ? 1 : 0, cfg.check, o);
+    }
   }
 }
 

@@ -435,10 +435,15 @@ fir_status fir_batch_get_launch(const fir_batch* batch, int* block, int* blocks_
  * every shape up to the order of the float atomic additions. */
 fir_status fir_batch_set_bundle(fir_batch* batch, int axial_tile);
 fir_status fir_batch_get_bundle(const fir_batch* batch, int* axial_tile);
-/* Autotuner: times the projector of step 0 (all problems' first subsets) for
- * each candidate launch shape (bundle shape, block size, residency, grab)
- * and keeps the fastest; *best_ms (may be NULL) receives its time.  It uses
- * the current images without changing them. */
+/* Autotuner: times the batched projector of the first step that has one
+ * (all batched problems' first subsets) for each candidate launch shape
+ * (bundle shape, block size, residency, grab) and keeps the fastest; *best_ms
+ * (may be NULL) receives its time.  It uses the current images without
+ * changing them.  A problem with at least 2^22 LORs per subset, or whose
+ * volume fits L2 only as float image and accumulator, is not batched: its
+ * projector runs as fir_osem's does, in launches of its own within each step,
+ * and the launch shape does not apply to it.  With no batched problem the
+ * tuner times nothing, reports no candidates and *best_ms = 0. */
 fir_status fir_batch_tune(fir_batch* batch, double* best_ms);
 /* The candidates of the last fir_batch_tune with their times: *n receives
  * their number; the first `max` are written to the arrays (each may be

@@ -10,6 +10,10 @@ of the other parity tests:
   * backprojection and sensitivity: relative L2 <= 1e-6, per voxel <= 1e-5 of
     the maximum;
   * OSEM, plain and batched: relative L2 <= 1e-4 against the oracle.
+A mid-size volume that only fits L2 as float image and accumulator, one
+orientation at a time, runs the fused kernel as two launches; it is checked
+against the deterministic mode (1e-6 relative L2) and, batched beside a small
+problem, against fir_osem (1e-5).
 """
 import numpy as np
 import pytest
@@ -132,3 +136,90 @@ def test_frames_match_single_frame(gpu_ctx_factory, name):
             ctx.backward(p, q[f].contiguous(), v, wb, 1)
             torch.cuda.synchronize()
             assert_scatter_close(b[f].cpu().numpy(), wb.cpu().numpy().astype(np.float64))
+
+
+def mid_volume():
+    """A volume whose double copy and accumulator (12 B per voxel) overflow the
+    device's L2 while the float image and accumulator (8 B) fit: the fused
+    kernel then gathers floats, in two launches, one per orientation, each
+    with its own (exchanged) float image and accumulator.  Unequal sizes, not
+    multiples of the 32-voxel tiles; sub-millimetre voxels, so exact geometry."""
+    l2 = torch.cuda.get_device_properties(0).L2_cache_size
+    nx, ny = 331, 287
+    nz = int(round(l2 / 9.5 / (nx * ny)))
+    n = nx * ny * nz
+    assert 8 * n <= l2 < 12 * n
+    return VolSpec.centred((nx, ny, nz), (0.3, 0.3, 24.0 / nz))
+
+
+def test_mid_volume_orientation_launches_match_deterministic():
+    """One subset's backprojected ratio from the two orientation launches
+    against the deterministic mode (double copy, one orientation, FIR's
+    summation order): within the float atomic order's 1e-6 relative L2."""
+    v = mid_volume()
+    s, p = geometry()
+    nb = capi.proj_geometry(p)["n_bins"]
+    g = torch.Generator(device="cuda").manual_seed(7)
+    img = torch.rand(v.shape_zyx, generator=g, device="cuda") + 0.5
+    y = torch.poisson(torch.full((nb,), 3.0, device="cuda"), generator=g)
+    got = torch.zeros_like(img)
+    want = torch.zeros_like(img)
+    ctx = capi.Context(s)
+    det = capi.Context(s)
+    try:
+        for c in (ctx, det):
+            c.set_option(capi.FIR_OPT_GEOMETRY, capi.FIR_GEOMETRY_EXACT)
+        det.set_option(capi.FIR_OPT_BACKPROJ_MODE, capi.FIR_BACKPROJ_DETERMINISTIC)
+        ctx.ratio_backprojection(p, y, v, img, got, 4, 1)
+        det.ratio_backprojection(p, y, v, img, want, 4, 1)
+        torch.cuda.synchronize()
+    finally:
+        det.close()
+        ctx.close()
+    assert float(want.max()) > 0
+    assert_scatter_close(got.cpu().numpy(), want.cpu().numpy().astype(np.float64))
+
+
+def test_mid_volume_batched_osem_matches_plain():
+    """In a batch, the mid-size problem runs fir_osem's kernel in launches of
+    its own (two per step, one per orientation) beside the batched projector
+    of a small problem: one OSEM iteration of both, tuned and captured as a
+    graph, against fir_osem on each."""
+    vols = [mid_volume(), VOLS["wide_x"]]
+    s, p = geometry()
+    nb = capi.proj_geometry(p)["n_bins"]
+    prm = OSEMParams(n_iterations=1, n_subsets=4, convolution_interval=1, fwhm_xyz=[1.0, 1.0, 1.0])
+    ctx = capi.Context(s)
+    ctx.set_option(capi.FIR_OPT_GEOMETRY, capi.FIR_GEOMETRY_EXACT)
+    batch = None
+    try:
+        data, want = [], []
+        for k, v in enumerate(vols):
+            x = torch.rand(v.shape_zyx, generator=torch.Generator(device="cuda").manual_seed(8 + k), device="cuda")
+            ax = torch.empty(nb, device="cuda")
+            ctx.forward(v, x, p, ax)
+            y = torch.poisson(ax * (2e6 / float(ax.double().sum())))
+            sens = torch.empty((prm.n_subsets,) + tuple(v.shape_zyx), device="cuda")
+            ctx.sensitivity(p, v, sens, prm.n_subsets)
+            plain = torch.ones(v.shape_zyx, device="cuda")
+            ctx.osem(p, y, v, plain, sens, prm)
+            data.append((y, sens))
+            want.append(plain.cpu().numpy())
+        batch = capi.Batch(ctx, [(s, p, v, prm) for v in vols])
+        for k, v in enumerate(vols):
+            batch.set_data(k, *data[k])
+            batch.set_image(k, np.ones(v.shape_zyx, np.float32))
+        n_steps, launches = batch.schedule()
+        # prepare, then per sub-iteration: the batched projector, two direct
+        # projector launches, the EM update and the three filter passes
+        assert (n_steps, launches) == (prm.n_subsets, 1 + prm.n_subsets * 7)
+        assert batch.tune() > 0 and len(batch.tune_report()) == 39
+        batch.osem(use_graph=True)
+        for k, v in enumerate(vols):
+            got = batch.get_image(k)
+            assert np.isfinite(got).all() and float(want[k].max()) > 0
+            assert rel_l2(got, want[k]) <= 1e-5, k
+    finally:
+        if batch is not None:
+            batch.close()
+        ctx.close()

@@ -12,9 +12,11 @@ real extents:
 * one OSEM iteration (32 subsets) run as one captured graph (a batch of one
   problem) matches fir_osem within 1e-5 relative L2;
 * the volume's double copy does not fit in L2 beside the accumulator, so the
-  fused kernel gathers the float image: one subset's backprojected ratio
-  matches the deterministic mode, which gathers the double copy and sums in
-  FIR's order, within the 1e-6 relative L2 of float atomic order.
+  fused kernel gathers the float image, in two launches that each take the
+  LORs of one orientation with their own (x/y-exchanged) image and
+  accumulator: one subset's backprojected ratio matches the deterministic
+  mode, which gathers the double copy and sums in FIR's order, within the
+  1e-6 relative L2 of float atomic order.
 """
 import numpy as np
 import pytest
