@@ -196,3 +196,46 @@ def test_batch_errors():
         capi.Batch(ctx, [(ws[1].scanner, ws[0].proj, ws[0].vol, ws[0].osem)])
     batch.close()
     ctx.close()
+
+
+def test_problem_with_large_subsets_runs_single_problem_kernel():
+    """A problem with 2^22 or more LORs per subset (the clinical scanner, 4
+    subsets) is not batched: each step runs fir_osem's kernel for it, with its
+    descriptor as kernel parameters, beside the batched launch of a small
+    problem.  Both images match fir_osem, as a graph and as direct launches,
+    and a new bias sinogram reaches the single-problem launches of the next
+    graph (the captured graph holds the old pointer, so it is rebuilt)."""
+    base = workloads.clinical()
+    big = workloads.Workload(
+        name="wide_subsets", scanner=base.scanner, proj=base.proj,
+        vol=VolSpec.centred((64, 64, 16), (4.0, 4.0, 4.0)),
+        osem=OSEMParams(n_iterations=1, n_subsets=4, convolution_interval=1, fwhm_xyz=[4.0, 4.0, 4.0]),
+        counts=2e6, seed=7, kind="cylinder", extra={"cyl_radius": 80.0})
+    assert capi.proj_geometry(big.proj)["n_bins"] // big.osem.n_subsets >= 1 << 22
+    ws = [big, mixed_problems()[0]]
+    ctx, batch, data = build(ws, bias_for=(0,))
+    try:
+        n_steps, launches = batch.schedule()
+        # prepare; per step: the batched projector (small problem, steps 1..8),
+        # the single-problem projector (big problem, steps 1..4), EM, filter
+        small = ws[1].osem.n_iterations * ws[1].osem.n_subsets
+        assert n_steps == small
+        assert launches == 1 + big.osem.n_subsets * (1 + 1 + 1 + 3) + (small - big.osem.n_subsets) * (1 + 1 + 3)
+        want = plain(ws, data)
+        for use_graph in (True, False):
+            reset(batch, ws)
+            batch.osem(use_graph=use_graph)
+            for k in range(len(ws)):
+                got = batch.get_image(k)
+                assert rel(got, want[k]) <= TOL_ATOMIC, (use_graph, k)
+        y, sens, _ = data[0]
+        bias = torch.full_like(y, 0.2)
+        batch.set_data(0, y, sens, bias)
+        want0 = plain([big], [(y, sens, bias)])[0]
+        reset(batch, ws)
+        batch.osem(use_graph=True)
+        assert rel(batch.get_image(0), want0) <= TOL_ATOMIC
+        assert rel(want0, want[0]) > 10 * TOL_ATOMIC  # the new bias changes the image
+    finally:
+        batch.close()
+        ctx.close()
