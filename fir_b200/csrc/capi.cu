@@ -530,9 +530,11 @@ void backproject_subset(fir_ctx& c, const Grid& g, const Sino& s, const Tables& 
 // ratio kernel followed by the ordered scatter.  The fused kernel reads and
 // accumulates LORs that run mostly along x in images with x and y exchanged
 // (double copy and accumulator in context scratch); the accumulator is added
-// back into bp after the kernel.
-void ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, const float* img,
-                       const float* sino, const float* mult, const float* bias, float* bp, long long nvox)
+// back into bp after the kernel, or, with defer_merge, returned (null: none)
+// for the caller to add (launch_em_update_oriented).
+const float* ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, const float* img,
+                               const float* sino, const float* mult, const float* bias, float* bp, long long nvox,
+                               bool defer_merge = false)
 {
   if (c.traversal == FIR_TRAVERSAL_FLOAT && c.backproj == FIR_BACKPROJ_ATOMIC && mult == nullptr &&
       c.step_limit == 0)
@@ -553,12 +555,16 @@ void ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t
     timed_launch(c, [&] {
       launch_osem_subset_float(g, s, t, img, img_t, sino, bias, bp, bp_t, c.skip_zero != 0, cfg_of(c));
     });
+    if (bp_t != nullptr && defer_merge)
+    {
+      return bp_t;
+    }
     if (bp_t != nullptr)
     {
       launch_merge_oriented(g.nx, g.ny, g.nz, bp, bp_t, cfg_of(c));
       after_launch(c);
     }
-    return;
+    return nullptr;
   }
   if (c.backproj == FIR_BACKPROJ_DETERMINISTIC)
   {
@@ -569,7 +575,7 @@ void ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t
     int* counts = reinterpret_cast<int*>(ratio + ne);
     timed_launch(c, [&] { launch_ratio(g, s, t, wimg, sino, mult, bias, ratio, counts, cfg_of(c)); });
     det_backproject(c, g, s, t, ratio, true, bp, nvox, counts);
-    return;
+    return nullptr;
   }
   if (!use_exchanged(c, g))
   {
@@ -588,15 +594,19 @@ void ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t
         launch_osem_subset_float_image(g, s, t, img, img_t, sino, mult, bias, bp, bp_t, c.skip_zero != 0,
                                        cfg_of(c));
       });
+      if (defer_merge)
+      {
+        return bp_t;
+      }
       launch_merge_oriented(g.nx, g.ny, g.nz, bp, bp_t, cfg_of(c));
       after_launch(c);
-      return;
+      return nullptr;
     }
     const double* wimg = widen(c, img, nvox);
     timed_launch(c, [&] {
       launch_osem_subset(g, s, t, wimg, nullptr, sino, mult, bias, bp, nullptr, c.skip_zero != 0, cfg_of(c));
     });
-    return;
+    return nullptr;
   }
   const size_t n = (size_t)nvox;
   double* wimg = static_cast<double*>(c.wide.ensure(n * sizeof(double)));
@@ -608,8 +618,13 @@ void ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t
   timed_launch(c, [&] {
     launch_osem_subset(g, s, t, wimg, wimg_t, sino, mult, bias, bp, bp_t, c.skip_zero != 0, cfg_of(c));
   });
+  if (defer_merge)
+  {
+    return bp_t;
+  }
   launch_merge_oriented(g.nx, g.ny, g.nz, bp, bp_t, cfg_of(c));
   after_launch(c);
+  return nullptr;
 }
 
 Tables tables_of(fir_ctx& c, const ProjInfo& p)
@@ -982,8 +997,15 @@ void osem_subiteration_device(fir_ctx& c, const ProjInfo& p, const Tables& t, co
   float* bp = static_cast<float*>(c.bp.ensure((size_t)v.nvox * sizeof(float)));
   cuda_ok(cudaMemsetAsync(bp, 0, (size_t)v.nvox * sizeof(float), c.stream), "cudaMemsetAsync");
   const Sino s = sino_of(p, prm->n_subsets, subset);
-  ratio_backproject(c, g, s, t, img, sino, mult, bias, bp, v.nvox);
-  launch_em_update(v.nvox, img, bp, sens_frame, cfg_of(c));
+  const float* bp_t = ratio_backproject(c, g, s, t, img, sino, mult, bias, bp, v.nvox, true);
+  if (bp_t != nullptr)
+  {
+    launch_em_update_oriented(g.nx, g.ny, g.nz, img, bp, bp_t, sens_frame, cfg_of(c));
+  }
+  else
+  {
+    launch_em_update(v.nvox, img, bp, sens_frame, cfg_of(c));
+  }
   after_launch(c);
   const bool conv = prm->convolution_interval > 0 && prm->fwhm_xyz[0] > 0.0 && prm->fwhm_xyz[1] > 0.0 &&
                     prm->fwhm_xyz[2] > 0.0;

@@ -137,45 +137,92 @@ __global__ void __launch_bounds__(kTile * kTileRows) k_merge_oriented(int nx, in
   }
 }
 
+// k_em_update with the exchanged accumulator added first: b = bp[z][y][x] +
+// bp_t[z][x][y] (the float addition of k_merge_oriented), then the gated
+// division and product of k_em_update; bp is left holding the quotient.
+__global__ void __launch_bounds__(kTile * kTileRows) k_em_update_oriented(int nx, int ny, int nz,
+                                                                          float* __restrict__ img,
+                                                                          float* __restrict__ bp,
+                                                                          const float* __restrict__ bp_t,
+                                                                          const float* __restrict__ sens)
+{
+  __shared__ float tile[kTile][kTile + 1];
+  const int x0 = blockIdx.x * kTile, y0 = blockIdx.y * kTile;
+  for (int z = blockIdx.z; z < nz; z += gridDim.z)
+  {
+    const size_t plane = (size_t)nx * ny * z;
+    for (int j = threadIdx.y; j < kTile; j += kTileRows)
+    {
+      const int x = x0 + j, y = y0 + threadIdx.x;
+      if (x < nx && y < ny)
+      {
+        tile[j][threadIdx.x] = bp_t[plane + (size_t)x * ny + y];
+      }
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < kTile; j += kTileRows)
+    {
+      const int y = y0 + j, x = x0 + threadIdx.x;
+      if (x < nx && y < ny)
+      {
+        const size_t k = plane + (size_t)y * nx + x;
+        const float b = __fadd_rn(bp[k], tile[threadIdx.x][j]);
+        const float sv = __ldg(sens + k);
+        const float q = ((double)b > kEps && (double)sv > kEps) ? __fdiv_rn(b, sv) : 0.0f;
+        const float v = img[k];
+        img[k] = ((double)v > kEps && (double)q > kEps) ? __fmul_rn(v, q) : 0.0f;
+        bp[k] = q;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 dim3 plane_tiles(int nx, int ny, int nz)
 {
   return dim3((unsigned)((nx + kTile - 1) / kTile), (unsigned)((ny + kTile - 1) / kTile),
               (unsigned)(nz < 65535 ? nz : 65535));
 }
 
-// One pass of operations::convolve (operations.cc:84-156): sum and weight
-// norm over the in-bounds taps, accumulated in float in tap order, then
-// sum / norm.
-__global__ void k_conv_pass(int nx, int ny, int nz, int axis, Taps taps, const float* __restrict__ in,
-                            float* __restrict__ out)
+// One pass of operations::convolve (operations.cc:84-156) along AXIS: sum
+// and weight norm over the in-bounds taps, accumulated in float in tap order,
+// then sum / norm.  Threads cover the xy plane (blockIdx.x) of slices
+// blockIdx.y, blockIdx.y + gridDim.y, ...; volumes hold fewer than 2^31
+// voxels (checked on the host), so 32-bit indices suffice and x, y come from
+// one division.
+template<int AXIS>
+__global__ void __launch_bounds__(256) k_conv_pass(int nx, int ny, int nz, Taps taps, const float* __restrict__ in,
+                                                   float* __restrict__ out)
 {
-  // volumes hold fewer than 2^31 voxels (checked on the host), so the
-  // coordinates come from 32-bit divisions
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nx * ny * nz)
+  const int nxy = nx * ny;
+  const int ixy = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ixy >= nxy)
   {
     return;
   }
-  const int x = i % nx;
-  const int y = (i / nx) % ny;
-  const int z = i / (nx * ny);
-  const int coord = axis == 0 ? x : (axis == 1 ? y : z);
-  const int len = axis == 0 ? nx : (axis == 1 ? ny : nz);
-  const int stride = axis == 0 ? 1 : (axis == 1 ? nx : nx * ny);
-  float sum = 0.0f, norm = 0.0f;
-  for (int k = -taps.half; k <= taps.half; ++k)
+  const int y = ixy / nx;
+  const int x = ixy - y * nx;
+  const int len = AXIS == 0 ? nx : (AXIS == 1 ? ny : nz);
+  const int stride = AXIS == 0 ? 1 : (AXIS == 1 ? nx : nxy);
+  for (int z = blockIdx.y; z < nz; z += gridDim.y)
   {
-    const int c = coord + k;
-    if (c >= 0 && c < len)
+    const int i = z * nxy + ixy;
+    const int coord = AXIS == 0 ? x : (AXIS == 1 ? y : z);
+    float sum = 0.0f, norm = 0.0f;
+    for (int k = -taps.half; k <= taps.half; ++k)
     {
-      const float kv = taps.w[taps.half + k];
-      sum = __fadd_rn(sum, __fmul_rn(kv, __ldg(in + i + k * stride)));
-      norm = __fadd_rn(norm, kv);
+      const int c = coord + k;
+      if (c >= 0 && c < len)
+      {
+        const float kv = taps.w[taps.half + k];
+        sum = __fadd_rn(sum, __fmul_rn(kv, __ldg(in + i + k * stride)));
+        norm = __fadd_rn(norm, kv);
+      }
     }
-  }
-  if (norm > 0.0f)
-  {
-    out[i] = __fdiv_rn(sum, norm);
+    if (norm > 0.0f)
+    {
+      out[i] = __fdiv_rn(sum, norm);
+    }
   }
 }
 
@@ -369,13 +416,36 @@ void launch_merge_oriented(int nx, int ny, int nz, float* bp, const float* bp_t,
   }
 }
 
+void launch_em_update_oriented(int nx, int ny, int nz, float* img, float* bp, const float* bp_t, const float* sens,
+                               const LaunchCfg& cfg)
+{
+  if ((long long)nx * ny * nz > 0)
+  {
+    k_em_update_oriented<<<plane_tiles(nx, ny, nz), dim3(kTile, kTileRows), 0, cfg.stream>>>(nx, ny, nz, img, bp,
+                                                                                             bp_t, sens);
+  }
+}
+
 void launch_conv_pass(int nx, int ny, int nz, int axis, const Taps& taps, const float* in, float* out,
                       const LaunchCfg& cfg)
 {
   const long long n = (long long)nx * ny * nz;
-  if (n > 0)
+  if (n <= 0)
   {
-    k_conv_pass<<<blocks_for(n), kBlock, 0, cfg.stream>>>(nx, ny, nz, axis, taps, in, out);
+    return;
+  }
+  const dim3 grid(blocks_for((long long)nx * ny), (unsigned)(nz < 65535 ? nz : 65535));
+  if (axis == 0)
+  {
+    k_conv_pass<0><<<grid, kBlock, 0, cfg.stream>>>(nx, ny, nz, taps, in, out);
+  }
+  else if (axis == 1)
+  {
+    k_conv_pass<1><<<grid, kBlock, 0, cfg.stream>>>(nx, ny, nz, taps, in, out);
+  }
+  else
+  {
+    k_conv_pass<2><<<grid, kBlock, 0, cfg.stream>>>(nx, ny, nz, taps, in, out);
   }
 }
 

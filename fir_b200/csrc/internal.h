@@ -87,6 +87,10 @@ struct Taps
   float w[2 * kMaxHalfTaps + 1];
 };
 void launch_em_update(long long n, float* img, float* bp, const float* sens, const LaunchCfg& cfg);
+// The same after adding the x/y-exchanged accumulator bp_t into bp (one
+// launch in place of launch_merge_oriented and launch_em_update).
+void launch_em_update_oriented(int nx, int ny, int nz, float* img, float* bp, const float* bp_t, const float* sens,
+                               const LaunchCfg& cfg);
 void launch_em_update_image_first(long long n, float* img, const float* bp, const float* sens,
                                   const LaunchCfg& cfg);
 // Exact widening of a float image to double for the projector gathers.
