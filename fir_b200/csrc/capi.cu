@@ -525,6 +525,25 @@ void backproject_subset(fir_ctx& c, const Grid& g, const Sino& s, const Tables& 
   }
 }
 
+// s with the compacted list of its bins whose measured value is not 0
+// (FIR_OPT_SKIP_ZERO_BINS), built on the context stream in context scratch.
+Sino nonzero_bins(fir_ctx& c, const Sino& s, const float* sino)
+{
+  size_t temp = 0;
+  cuda_ok(launch_nonzero_list(s, sino, nullptr, nullptr, nullptr, &temp, cfg_of(c)), "cub::DeviceSelect");
+  const size_t list_bytes = ((size_t)s.n_enum * sizeof(int) + 255) / 256 * 256;
+  auto* base = static_cast<unsigned char*>(c.compact.ensure(list_bytes + 256 + temp));
+  int* list = reinterpret_cast<int*>(base);
+  int* count = reinterpret_cast<int*>(base + list_bytes);
+  cuda_ok(launch_nonzero_list(s, sino, list, count, base + list_bytes + 256, &temp, cfg_of(c)),
+          "cub::DeviceSelect");
+  after_launch(c);
+  Sino out = s;
+  out.list = list;
+  out.list_n = count;
+  return out;
+}
+
 // bp (zeroed by the caller) += backprojection of sino / (projection of img +
 // bias) over the subset of s: the fused kernel, or in deterministic mode the
 // ratio kernel followed by the ordered scatter.  The fused kernel reads and
@@ -532,10 +551,13 @@ void backproject_subset(fir_ctx& c, const Grid& g, const Sino& s, const Tables& 
 // (double copy and accumulator in context scratch); the accumulator is added
 // back into bp after the kernel, or, with defer_merge, returned (null: none)
 // for the caller to add (launch_em_update_oriented).
-const float* ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, const float* img,
+const float* ratio_backproject(fir_ctx& c, const Grid& g, const Sino& s_all, const Tables& t, const float* img,
                                const float* sino, const float* mult, const float* bias, float* bp, long long nvox,
                                bool defer_merge = false)
 {
+  // skipped bins: listed out of the atomic kernels' enumeration
+  const bool listed = c.skip_zero != 0 && c.backproj == FIR_BACKPROJ_ATOMIC && s_all.n_enum > 0;
+  const Sino s = listed ? nonzero_bins(c, s_all, sino) : s_all;
   if (c.traversal == FIR_TRAVERSAL_FLOAT && c.backproj == FIR_BACKPROJ_ATOMIC && mult == nullptr &&
       c.step_limit == 0)
   {
@@ -1396,7 +1418,8 @@ fir_status fir_ctx_destroy(fir_ctx* c)
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     for (DevBuf* b : {&c->xy, &c->z, &c->check, &c->bp, &c->conv1, &c->conv2, &c->conv_copy, &c->mu, &c->wide,
-                      &c->det, &c->det_pairs, &c->ratio, &c->frames_il, &c->frames_acc, &c->psf_blur, &c->psf_sens, &c->rebin})
+                      &c->det, &c->det_pairs, &c->ratio, &c->frames_il, &c->frames_acc, &c->psf_blur, &c->psf_sens, &c->rebin,
+                      &c->wide_t, &c->bp_t, &c->img_t, &c->frames_il_t, &c->frames_acc_t, &c->compact})
     {
       b->release();
     }

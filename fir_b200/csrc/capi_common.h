@@ -161,6 +161,7 @@ struct fir_ctx
   fir::abi::DevBuf bp, conv1, conv2, conv_copy, mu, wide, det, det_pairs, ratio, frames_il, frames_acc, psf_blur, psf_sens, rebin;
   fir::abi::DevBuf wide_t, bp_t;  // x/y-exchanged double image and accumulator of the fused kernel
   fir::abi::DevBuf img_t;         // x/y-exchanged float image (float traversal, float gathers)
+  fir::abi::DevBuf compact;       // non-zero bins of a subset (FIR_OPT_SKIP_ZERO_BINS) and CUB scratch
   fir::abi::DevBuf frames_il_t, frames_acc_t;  // the same for the multi-frame projectors
   std::vector<fir::abi::DevBuf> staging;
 

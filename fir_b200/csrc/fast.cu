@@ -149,7 +149,8 @@ __global__ void __launch_bounds__(256, 4) k_osem_subset_float(Grid g, Sino s, Ta
                                                             int skip_zero, int* check)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = i < s.n_enum;
+  bool valid = false;
+  const int ie = enum_index(s, i, valid);
   Lor l{};
   Walk w{};
   bool go = false;
@@ -157,7 +158,7 @@ __global__ void __launch_bounds__(256, 4) k_osem_subset_float(Grid g, Sino s, Ta
   float y = 0.0f;
   if (valid)
   {
-    l = decode_bin(s, i);
+    l = decode_bin(s, ie);
     y = __ldg(sino + l.bin);
     if (!(skip_zero && y == 0.0f))
     {

@@ -49,6 +49,11 @@ void launch_osem_subset(const Grid& g, const Sino& s, const Tables& t, const dou
 void launch_osem_subset_float_image(const Grid& g, const Sino& s, const Tables& t, const float* img,
                                     const float* img_t, const float* sino, const float* mult, const float* bias,
                                     float* bp, float* bp_t, bool skip_zero, const LaunchCfg& cfg);
+// compact.cu: the enumerated indices of s (list null) whose bin of sino is
+// not 0, ascending, into list (s.n_enum entries), their number into *count
+// (device memory).  With temp null only *temp_bytes is set (CUB convention).
+cudaError_t launch_nonzero_list(const Sino& s, const float* sino, int* list, int* count, void* temp,
+                                size_t* temp_bytes, const LaunchCfg& cfg);
 // fast.cu: the opt-in float traversal of the fused OSEM kernel.
 void launch_osem_subset_float(const Grid& g, const Sino& s, const Tables& t, const float* img, const float* img_t,
                               const float* sino, const float* bias, float* bp, float* bp_t, bool skip_zero,

@@ -45,7 +45,8 @@ __device__ __forceinline__ void osem_lor_body(const Grid& g, const Sino& s, int 
                                               const float* __restrict__ bias, float* bp, float* bp_t,
                                               bool skip_zero, int i, int* check, int orient = -1)
 {
-  const bool valid = i < s.n_enum;
+  bool valid = false;
+  const int ie = enum_index(s, i, valid);
   Lor l{};
   Walk w{};
   bool go = false;
@@ -53,7 +54,7 @@ __device__ __forceinline__ void osem_lor_body(const Grid& g, const Sino& s, int 
   float y = 0.0f;
   if (valid)
   {
-    l = decode_bin(s, i, subset);
+    l = decode_bin(s, ie, subset);
     y = __ldg(sino + l.bin);
     // With y == 0 the ratio is exactly 0 whatever the estimate, so the bin
     // contributes nothing: skipping it is exact.

@@ -43,6 +43,10 @@ struct Sino
   int seg_base[kMaxSegments + 1];      // first flat bin of each segment (file order)
   int enum_base[kMaxSegments + 1];     // first enumerated index of each segment
   int n_axial[kMaxSegments];
+  // null, or a compacted enumeration: thread i < *list_n takes the enumerated
+  // index list[i] (ascending), so that skipped bins take no lanes
+  const int* list;
+  const int* list_n;
 };
 
 struct Tables
@@ -91,6 +95,19 @@ __device__ __forceinline__ Lor decode_bin(const Sino& s, int i, int subset)
 }
 
 __device__ __forceinline__ Lor decode_bin(const Sino& s, int i) { return decode_bin(s, i, s.subset); }
+
+// The enumerated index that thread i traces: i itself, or the i-th entry of
+// the compacted list; valid is false past the end of either.
+__device__ __forceinline__ int enum_index(const Sino& s, int i, bool& valid)
+{
+  if (s.list == nullptr)
+  {
+    valid = i < s.n_enum;
+    return i;
+  }
+  valid = i < __ldg(s.list_n);
+  return valid ? __ldg(s.list + i) : 0;
+}
 
 // ProjData::getCrystalAxialCoord (ProjData.cc:198-299): slice indices.
 __device__ __forceinline__ void crystal_axial(const Sino& s, int seg, int axial, int& a1, int& a2)
