@@ -504,27 +504,6 @@ Widened widen_for_projection(fir_ctx& c, const Grid& g, const float* img)
   return Widened{d, d_t};
 }
 
-// img += backprojection of sino (nullptr: all ones) over the subset of s, in
-// the atomic mode; LORs running mostly along x accumulate in an x/y-exchanged
-// scratch image that is added into img afterwards, while both fit in L2.
-void backproject_subset(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, const float* sino, float* img,
-                        bool skip_zero)
-{
-  float* img_t = nullptr;
-  const long long n = (long long)g.nxy * g.nz;
-  if (use_exchanged(c, g, 8.0))
-  {
-    img_t = static_cast<float*>(c.bp_t.ensure((size_t)n * sizeof(float)));
-    cuda_ok(cudaMemsetAsync(img_t, 0, (size_t)n * sizeof(float), c.stream), "cudaMemsetAsync");
-  }
-  timed_launch(c, [&] { launch_backward(g, s, t, sino, img, img_t, skip_zero, cfg_of(c)); });
-  if (img_t != nullptr)
-  {
-    launch_merge_oriented(g.nx, g.ny, g.nz, img, img_t, cfg_of(c));
-    after_launch(c);
-  }
-}
-
 // s with the compacted list of its bins whose measured value is not 0
 // (FIR_OPT_SKIP_ZERO_BINS), built on the context stream in context scratch.
 Sino nonzero_bins(fir_ctx& c, const Sino& s, const float* sino)
@@ -542,6 +521,29 @@ Sino nonzero_bins(fir_ctx& c, const Sino& s, const float* sino)
   out.list = list;
   out.list_n = count;
   return out;
+}
+
+// img += backprojection of sino (nullptr: all ones) over the subset of s, in
+// the atomic mode; LORs running mostly along x accumulate in an x/y-exchanged
+// scratch image that is added into img afterwards, while both fit in L2.
+void backproject_subset(fir_ctx& c, const Grid& g, const Sino& s, const Tables& t, const float* sino, float* img,
+                        bool skip_zero)
+{
+  float* img_t = nullptr;
+  const long long n = (long long)g.nxy * g.nz;
+  if (use_exchanged(c, g, 8.0))
+  {
+    img_t = static_cast<float*>(c.bp_t.ensure((size_t)n * sizeof(float)));
+    cuda_ok(cudaMemsetAsync(img_t, 0, (size_t)n * sizeof(float), c.stream), "cudaMemsetAsync");
+  }
+  // skipped bins: listed out of the enumeration
+  const Sino sl = skip_zero && sino != nullptr && s.n_enum > 0 ? nonzero_bins(c, s, sino) : s;
+  timed_launch(c, [&] { launch_backward(g, sl, t, sino, img, img_t, skip_zero, cfg_of(c)); });
+  if (img_t != nullptr)
+  {
+    launch_merge_oriented(g.nx, g.ny, g.nz, img, img_t, cfg_of(c));
+    after_launch(c);
+  }
 }
 
 // bp (zeroed by the caller) += backprojection of sino / (projection of img +

@@ -85,9 +85,11 @@ __global__ void __launch_bounds__(256) k_backward(Grid g, Sino s, Tables t,
   bool go = false;
   bool tr = false;
   double v = 0.0;
-  if (i < s.n_enum)
+  bool valid = false;
+  const int ie = enum_index(s, i, valid);
+  if (valid)
   {
-    const Lor l = decode_bin(s, i);
+    const Lor l = decode_bin(s, ie);
     const float val = sino != nullptr ? __ldg(sino + l.bin) : 1.0f;
     v = (double)val;
     // with val == 0 every contribution is exactly 0

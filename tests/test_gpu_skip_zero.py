@@ -7,7 +7,8 @@ list of the subset's non-zero bins.  Bars: one sub-iteration with and
 without the option within 1e-6 relative L2, per voxel within 1e-5 of the
 maximum; three OSEM iterations against the oracle within 1e-4.  Covered: the
 exact traversal (exchanged double images), the opt-in float traversal, a
-sinogram that is mostly zeros, and one that is all zeros."""
+sinogram that is mostly zeros, and one that is all zeros; and the plain
+backprojector (fir_backward), which takes the same list."""
 import numpy as np
 import pytest
 import torch
@@ -76,3 +77,25 @@ def test_skip_osem_matches_oracle(restated):
     want = restated.osem(w.scanner, w.proj, w.vol, y.cpu().numpy(), np.ones(w.vol.shape_zyx, np.float32),
                          sens.cpu().numpy(), w.osem)
     assert rel_l2(got, want) <= 1e-4
+
+
+@pytest.mark.parametrize("keep", [1.0, 0.3])
+def test_skip_backward_matches_full_enumeration(keep):
+    """fir_backward of a measured sinogram, per subset, with and without the
+    option (the plain backprojector takes the same compacted list)."""
+    w = workloads.small()
+    with capi.Context(w.scanner) as ctx:
+        y, _ = workloads.measured_on_gpu(ctx, w, DEV, attenuation=True)
+        y = sparse(y, keep, 5) if keep < 1.0 else y
+        nsub = w.osem.n_subsets
+        out = []
+        for skip in (0, 1):
+            ctx.set_option(capi.FIR_OPT_SKIP_ZERO_BINS, skip)
+            bp = torch.empty((nsub,) + tuple(w.vol.shape_zyx), device="cuda")
+            ctx.backward(w.proj, y, w.vol, bp, nsub)
+            torch.cuda.synchronize()
+            out.append(bp.cpu().numpy())
+    want, got = out
+    assert float(want.max()) > 0
+    assert rel_l2(got, want) <= 1e-6
+    assert np.abs(got - want).max() <= 1e-5 * np.abs(want).max()
