@@ -709,6 +709,10 @@ Grid grid_of(const fir_ctx& c, const VolInfo& v)
       g.ext[d] = vox[d];
     }
   }
+  for (int d = 0; d < 3; ++d)
+  {
+    g.rext[d] = 1.0 / g.ext[d];  // IEEE division: RN(1 / ext)
+  }
   const double depth = v.d.nz * v.d.voxel_z;
   g.low[0] = v.d.offset_x - v.d.voxel_x / 2;
   g.low[1] = v.d.offset_y - v.d.voxel_y / 2;

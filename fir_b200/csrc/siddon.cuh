@@ -29,6 +29,7 @@ struct Grid
   double ext[3];   // step sizes: FIR's int-truncated extents, or the real ones
   double low[3];   // border planes: x,y = offset - voxel/2, z = offset - depth/2
   double high[3];  // low + n * voxel (real voxel extents, as in FIR)
+  double rext[3];  // RN(1 / ext)
 };
 
 // Sinogram enumeration for one launch.  Bins are enumerated segment by
@@ -65,6 +66,25 @@ __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a,
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+// RN(a / b) from rb = RN(1 / b).  q = RN(a rb) is within two ulps of a / b;
+// a correction by the remainder a - b q (one fused multiply-add) makes it
+// faithful, and a second correction then rounds it correctly by Markstein's
+// theorem (P. Markstein, IBM J. Res. Develop. 34(1), 1990: with y = RN(1/b)
+// and q faithful, RN(q + y (a - b q)) = RN(a / b)).  The theorem needs finite
+// operands far from overflow and underflow, as the traversal's finite ones
+// are.  An infinite operand makes a remainder NaN (inf * 0 or inf - inf);
+// for those operands RN(a rb) itself is the IEEE quotient (finite / inf =
+// signed 0, inf / finite = signed inf, inf / inf and NaN give NaN), and it
+// is returned instead.
+__device__ __forceinline__ double ddiv_r(double a, double b, double rb)
+{
+  const double q0 = __dmul_rn(a, rb);
+  double r = __fma_rn(-b, q0, a);
+  double q = __fma_rn(r, rb, q0);
+  r = __fma_rn(-b, q, a);
+  q = __fma_rn(r, rb, q);
+  return q == q ? q : q0;
+}
 
 // Enumerated index -> bin coordinates, for subset `subset` of s.n_subsets
 // (the enumeration bases depend only on the number of subsets).
@@ -278,17 +298,18 @@ __device__ __forceinline__ bool siddon_setup(const Grid& g, const double e[6], W
     double df = dsub(c2, c1);
     if (fabs(df) > kEps)
     {
+      const double rdf = __drcp_rn(df);
       if (df > 0)
       {
         dir[d] = 1;
-        smin[d] = ddiv(dsub(lo, c1), df);
-        smax[d] = ddiv(dsub(hi, c1), df);
+        smin[d] = ddiv_r(dsub(lo, c1), df, rdf);
+        smax[d] = ddiv_r(dsub(hi, c1), df, rdf);
       }
       else
       {
         dir[d] = -1;
-        smin[d] = ddiv(dsub(hi, c1), df);
-        smax[d] = ddiv(dsub(lo, c1), df);
+        smin[d] = ddiv_r(dsub(hi, c1), df, rdf);
+        smax[d] = ddiv_r(dsub(lo, c1), df, rdf);
       }
       snext[d] = 0.0;
     }
@@ -320,23 +341,26 @@ __device__ __forceinline__ bool siddon_setup(const Grid& g, const double e[6], W
   const int n[3] = {g.nx, g.ny, g.nz};
   const int stride[3] = {transpose ? g.ny : 1, transpose ? 1 : g.nx, g.nxy};
   w.tr = transpose ? 1 : 0;
+  double rdiff[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d)
   {
-    w.da[d] = ddiv(g.ext[d], fabs(diff[d]));
+    // RN is symmetric, so ext / |diff| = |RN(ext / diff)|
+    rdiff[d] = __drcp_rn(diff[d]);
+    w.da[d] = fabs(ddiv_r(g.ext[d], diff[d], rdiff[d]));
   }
   w.d12 = __dsqrt_rn(dadd(dadd(dmul(diff[0], diff[0]), dmul(diff[1], diff[1])), dmul(diff[2], diff[2])));
   w.c = 0;
 #pragma unroll
   for (int d = 0; d < 3; ++d)
   {
-    int ind = __double2int_rz(ddiv(dsub(dadd(e[d], dmul(diff[d], w.amin)), g.low[d]), g.ext[d]));
+    int ind = __double2int_rz(ddiv_r(dsub(dadd(e[d], dmul(diff[d], w.amin)), g.low[d]), g.ext[d], g.rext[d]));
     ind = ind < n[d] - 1 ? ind : n[d] - 1;
     ind = ind > 0 ? ind : 0;
     double al = snext[d];
     if (al < 1.0)
     {
-      al = ddiv(dsub(dadd(g.low[d], dmul(g.ext[d], (double)ind)), e[d]), diff[d]);
+      al = ddiv_r(dsub(dadd(g.low[d], dmul(g.ext[d], (double)ind)), e[d]), diff[d], rdiff[d]);
     }
     if (dir[d] > 0)
     {

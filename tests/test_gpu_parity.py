@@ -101,6 +101,36 @@ def test_random_segments_bit_exact_both_geometries(gpu_ctx_factory, restated):
         assert_paths_equal(ctx.siddon_paths(v, segs), restated.siddon_paths(v, segs, truncate=trunc))
 
 
+def test_setup_divisions_bit_exact_near_parallel_and_wide_range(gpu_ctx_factory, restated):
+    """The set-up's quotients come from a correctly rounded reciprocal and two
+    fused multiply-add corrections; they must equal the oracle's IEEE
+    divisions.  Stress: segments within 1e-5..1e-2 mm of parallel to an axis
+    (reciprocals up to 1e5), end points from 1e-3 to 1e3 mm, odd voxel sizes."""
+    rng = np.random.default_rng(29)
+    v = VolSpec((37, 41, 23), (1.7, 2.3, 3.1), (-30.6, -46.0, -7.0))
+    n = 30000
+    a = rng.uniform(-1, 1, (n, 3)) * 10.0 ** rng.uniform(-3, 3, (n, 1))
+    b = rng.uniform(-1, 1, (n, 3)) * 10.0 ** rng.uniform(-3, 3, (n, 1))
+    for k in range(3):
+        sl = slice(k * n // 4, (k + 1) * n // 4)
+        sign = rng.choice([-1.0, 1.0], sl.stop - sl.start)
+        b[sl, k] = a[sl, k] + sign * 10.0 ** rng.uniform(-5, -2, sl.stop - sl.start) * 1.0001
+    segs = np.concatenate([a, b], axis=1)
+    # non-finite end points, where the quotient falls back to RN(a RN(1/b))
+    bad = np.tile(np.array([[-3.0, 2.0, 1.0, 9.0, -7.0, 4.0]]), (18, 1))
+    for k, val in enumerate((np.inf, -np.inf, np.nan)):
+        for c in range(6):
+            bad[k * 6 + c, c] = val
+    for mode, trunc in ((capi.FIR_GEOMETRY_REFERENCE, True), (capi.FIR_GEOMETRY_EXACT, False)):
+        ctx = gpu_ctx_factory()
+        ctx.set_option(capi.FIR_OPT_GEOMETRY, mode)
+        assert_paths_equal(ctx.siddon_paths(v, segs), restated.siddon_paths(v, segs, truncate=trunc))
+        got = ctx.siddon_paths(v, bad)
+        want = restated.siddon_paths(v, bad, truncate=trunc)
+        np.testing.assert_array_equal(got[0], want[0])
+        np.testing.assert_array_equal(got[1], want[1])
+
+
 # ------------------------------------------------------------ projectors
 
 def test_forward_tiny_matches_fir_golden(gpu_ctx_factory):
