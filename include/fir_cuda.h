@@ -144,7 +144,11 @@ typedef enum fir_option
    * with FIR's rounding, reproducing a single-threaded FIR run. */
   FIR_OPT_BACKPROJ_MODE = 2,
   /* 1: skip sinogram bins whose value is exactly 0 in backprojection and
-   * OSEM (their contribution is exactly 0).  Default 0. */
+   * OSEM (their contribution is exactly 0).  Default 0.  In the atomic mode
+   * the OSEM sub-iteration and fir_backward first list a subset's non-zero
+   * bins on the device (5 bytes of context scratch per LOR of the subset)
+   * and trace only those; the result equals the full enumeration's up to the
+   * order of the float atomic additions. */
   FIR_OPT_SKIP_ZERO_BINS = 3,
   /* Threads per block of the projector kernels (32..256, multiple of 32);
    * 0 restores the default. */
